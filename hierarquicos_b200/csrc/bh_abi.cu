@@ -1,0 +1,549 @@
+// C ABI of the force engine: workspace management, the build/walk pipeline
+// and status reporting.  See include/hierarquicos_bh.h for the contract.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "bh_internal.cuh"
+
+using bh::Buffers;
+
+struct bh_system {
+  int device = 0;
+  Buffers b;
+  int64_t n = 0;
+  int built = 0;
+  int verify_pending = 0;
+  int order = 4;
+  int64_t stack_cap = 4096;
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_done = nullptr;
+  const double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
+  bh_params p{};
+};
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int set_err(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define BH_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return set_err(e_ == cudaErrorMemoryAllocation ? BH_ERR_NOMEM : BH_ERR_CUDA, "%s: %s", \
+                     #call, cudaGetErrorString(e_));                                         \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, int64_t count) {
+  if (count < 1) count = 1;
+  return cudaMalloc((void **)p, (size_t)count * sizeof(T));
+}
+
+void free_buffers(Buffers &b) {
+  void *ptrs[] = {b.hm, b.hx, b.hy, b.hz, b.hout, b.k0, b.k1, b.v0, b.v1, b.hist, b.partials,
+                  b.spos, b.bn_left, b.bn_right, b.bn_parent, b.bn_first, b.bn_last, b.bn_level,
+                  b.bn_flag, b.bin2cn, b.cn_bin, b.cn_meta, b.cn_child, b.cn_parent, b.cn_com,
+                  b.cn_quad, b.cn_oct, b.cn_fq, b.cn_fo, b.level_begin, b.gflag, b.gscan,
+                  b.g_first, b.scan_tmp, b.wstack, b.counters, b.stats, b.sc};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  if (b.sc_host) cudaFreeHost(b.sc_host);
+  b = Buffers();
+}
+
+int ensure_capacity(bh_system *s, int64_t n) {
+  Buffers &b = s->b;
+  if (b.cap >= n && b.wstack_cap >= s->stack_cap) return BH_OK;
+  if (b.cap >= n) {
+    // only the walk stack grows
+    if (b.wstack) cudaFree(b.wstack);
+    b.wstack = nullptr;
+    b.wstack_slots = bh::walk_slots();
+    BH_CUDA(dalloc(&b.wstack, b.wstack_slots * s->stack_cap));
+    b.wstack_cap = s->stack_cap;
+    return BH_OK;
+  }
+  free_buffers(b);
+  const int64_t c = n < 2 ? 2 : n;
+  BH_CUDA(dalloc(&b.k0, c)); BH_CUDA(dalloc(&b.k1, c));
+  BH_CUDA(dalloc(&b.v0, c)); BH_CUDA(dalloc(&b.v1, c));
+  b.hist_cap = bh::radix_hist_entries(c);
+  BH_CUDA(dalloc(&b.hist, b.hist_cap));
+  BH_CUDA(dalloc(&b.partials, 296 * 10));
+  BH_CUDA(dalloc(&b.spos, c));
+  BH_CUDA(dalloc(&b.bn_left, c)); BH_CUDA(dalloc(&b.bn_right, c)); BH_CUDA(dalloc(&b.bn_parent, c));
+  BH_CUDA(dalloc(&b.bn_first, c)); BH_CUDA(dalloc(&b.bn_last, c)); BH_CUDA(dalloc(&b.bn_level, c));
+  BH_CUDA(dalloc(&b.bn_flag, c)); BH_CUDA(dalloc(&b.bin2cn, c));
+  BH_CUDA(dalloc(&b.cn_bin, c)); BH_CUDA(dalloc(&b.cn_meta, c)); BH_CUDA(dalloc(&b.cn_child, 8 * c));
+  BH_CUDA(dalloc(&b.cn_parent, c)); BH_CUDA(dalloc(&b.cn_com, c));
+  BH_CUDA(dalloc(&b.cn_quad, 6 * c)); BH_CUDA(dalloc(&b.cn_oct, 14 * c));
+  BH_CUDA(dalloc(&b.cn_fq, 2 * c)); BH_CUDA(dalloc(&b.cn_fo, 4 * c));
+  BH_CUDA(dalloc(&b.level_begin, bh::kNumLevels + 2));
+  BH_CUDA(dalloc(&b.gflag, c + 1)); BH_CUDA(dalloc(&b.gscan, c + 1)); BH_CUDA(dalloc(&b.g_first, c + 1));
+  b.scan_tmp_cap = bh::scan_tmp_entries(c + 1);
+  BH_CUDA(dalloc(&b.scan_tmp, b.scan_tmp_cap));
+  b.wstack_slots = bh::walk_slots();
+  BH_CUDA(dalloc(&b.wstack, b.wstack_slots * s->stack_cap));
+  b.wstack_cap = s->stack_cap;
+  BH_CUDA(dalloc(&b.counters, 8));
+  BH_CUDA(dalloc(&b.stats, 4));
+  BH_CUDA(dalloc(&b.sc, 1));
+  BH_CUDA(cudaMallocHost((void **)&b.sc_host, sizeof(bh::Scalars)));
+  BH_CUDA(cudaMemset(b.sc, 0, sizeof(bh::Scalars)));
+  BH_CUDA(cudaMemset(b.stats, 0, 4 * sizeof(unsigned long long)));
+  b.cap = c;
+  return BH_OK;
+}
+
+int ensure_host_staging(bh_system *s, int64_t n) {
+  Buffers &b = s->b;
+  if (b.hm && b.cap >= n) return BH_OK;
+  if (b.hm) { cudaFree(b.hm); cudaFree(b.hx); cudaFree(b.hy); cudaFree(b.hz); cudaFree(b.hout); }
+  const int64_t c = b.cap;
+  BH_CUDA(dalloc(&b.hm, c)); BH_CUDA(dalloc(&b.hx, c)); BH_CUDA(dalloc(&b.hy, c));
+  BH_CUDA(dalloc(&b.hz, c)); BH_CUDA(dalloc(&b.hout, 3 * c));
+  return BH_OK;
+}
+
+int check_params(const bh_params *p, int64_t n) {
+  if (!p) return set_err(BH_ERR_INVALID, "params is NULL");
+  if (n < 1 || n > (int64_t)(1 << 30)) return set_err(BH_ERR_INVALID, "n=%lld out of range [1, 2^30]", (long long)n);
+  if (p->order != 1 && p->order != 4 && p->order != 8)
+    return set_err(BH_ERR_INVALID, "order must be 1, 4 or 8 (got %d)", p->order);
+  if (p->depth < 0 || p->depth > bh::kMaxDepth)
+    return set_err(BH_ERR_INVALID, "depth must be in 0..21 (got %d)", p->depth);
+  if (!(p->theta >= 0.0) || !isfinite(p->theta)) return set_err(BH_ERR_INVALID, "theta must be finite and >= 0");
+  if (!(p->eps >= 0.0) || !isfinite(p->eps)) return set_err(BH_ERR_INVALID, "eps must be finite and >= 0");
+  if (!isfinite(p->G)) return set_err(BH_ERR_INVALID, "G must be finite");
+  if (!(p->amp > 0.0) || !isfinite(p->amp)) return set_err(BH_ERR_INVALID, "amp must be > 0");
+  if (p->precision < 0 || p->precision > 2) return set_err(BH_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (p->group_size != 32 && p->group_size != 64) return set_err(BH_ERR_INVALID, "group_size must be 32 or 64");
+  if (p->leaf_cap < 1 || p->leaf_cap > 64) return set_err(BH_ERR_INVALID, "leaf_cap must be in 1..64");
+  if (p->out_kind != 0 && p->out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
+  if (p->com_mode != 0 && p->com_mode != 1) return set_err(BH_ERR_INVALID, "com_mode must be 0 or 1");
+  return BH_OK;
+}
+
+int status_from_device(bh_system *s, int ignore_stack) {
+  const bh::Scalars &h = *s->b.sc_host;
+  int e = h.err;
+  if (ignore_stack) e &= ~bh::kErrStackOverflow;
+  if (e & bh::kErrNonFinite)
+    return set_err(BH_ERR_NONFINITE, "non-finite position or mass, or total mass <= 0");
+  if (e & bh::kErrDuplicates)
+    return set_err(BH_ERR_DUPLICATES, "depth 0: coincident bodies never get distinct keys");
+  if (e & (bh::kErrIndex | bh::kErrChildren))
+    return set_err(BH_ERR_INTERNAL, "internal tree check failed (flags 0x%x)", e);
+  if (e & bh::kErrStackOverflow)
+    return set_err(BH_ERR_CAPACITY, "walk stack capacity %lld exceeded", (long long)s->stack_cap);
+  return BH_OK;
+}
+
+int read_scalars(bh_system *s, cudaStream_t st) {
+  BH_CUDA(cudaMemcpyAsync(s->b.sc_host, s->b.sc, sizeof(bh::Scalars), cudaMemcpyDeviceToHost, st));
+  BH_CUDA(cudaStreamSynchronize(st));
+  return BH_OK;
+}
+
+// keys (from scratch or from the scalars' centre of mass) -> sort -> octree ->
+// multipoles -> groups
+void enqueue_build(bh_system *s, int64_t n, int keys_from_scalars, cudaStream_t st) {
+  Buffers &b = s->b;
+  const bh_params &p = s->p;
+  const int L = p.depth;
+  if (keys_from_scalars)
+    bh::launch_keys_only(s->x, s->y, s->z, n, L, b, st);
+  else
+    bh::launch_keys(s->m, s->x, s->y, s->z, n, L, p.amp, p.com_mode, p.strict_keys, b, st, s->side,
+                    s->side_done);
+  const int bits = (L == 0) ? 3 * bh::kMaxDepth : 3 * L;
+  bh::radix_sort_pairs(b.k0, b.v0, b.k1, b.v1, n, nullptr, bits, b.hist, st);
+  if (L == 0) bh::launch_auto_depth(n, b, st);
+  bh::launch_gather(s->m, s->x, s->y, s->z, n, b, st);
+  if (n >= 2) {
+    bh::launch_build_tree(n, L, b, st);
+    bh::launch_upward(n, L, p.order, b, st);
+    bh::launch_groups(n, p.group_size, b, st);
+  }
+}
+
+bh::WalkParams walk_params(const bh_params *p, int order) {
+  bh::WalkParams w;
+  w.theta2 = p->theta * p->theta;
+  w.G = p->G;
+  w.eps2 = p->eps * p->eps;
+  w.order = p->order < order ? p->order : order;
+  w.out_kind = p->out_kind;
+  w.precision = p->precision;
+  w.group_size = p->group_size;
+  w.leaf_cap = p->leaf_cap;
+  w.count_stats = p->reserved[0];
+  return w;
+}
+
+std::mutex g_default_mu;
+bh_system *g_default[64] = {nullptr};
+
+int default_system(bh_system **out) {
+  int dev = 0;
+  BH_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_err(BH_ERR_INVALID, "device %d out of range", dev);
+  if (!g_default[dev]) {
+    int rc = bh_system_create(&g_default[dev], dev);
+    if (rc) return rc;
+  }
+  *out = g_default[dev];
+  return BH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void bh_params_default(bh_params *p) {
+  memset(p, 0, sizeof *p);
+  p->theta = 0.5;
+  p->G = 1.0;
+  p->eps = 0.0;
+  p->order = 4;
+  p->out_kind = 0;
+  p->depth = 21;
+  p->precision = BH_PREC_FP32;
+  p->amp = 1.2;
+  p->group_size = 64;
+  p->leaf_cap = 8;
+  p->com_mode = 1;
+  p->strict_keys = 1;
+}
+
+const char *bh_version(void) { return "hierarquicos-b200 0.1.0 (sm_100a)"; }
+
+int bh_last_error(char *buf, int len) {
+  if (buf && len > 0) {
+    strncpy(buf, g_err, (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)strlen(g_err);
+}
+
+int bh_system_create(bh_system **sys, int device) {
+  if (!sys) return set_err(BH_ERR_INVALID, "sys is NULL");
+  *sys = nullptr;
+  int ndev = 0;
+  BH_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return set_err(BH_ERR_INVALID, "no CUDA device %d", device);
+  BH_CUDA(cudaSetDevice(device));
+  bh_system *s = new bh_system();
+  s->device = device;
+  bh_params_default(&s->p);
+  if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->side_done, cudaEventDisableTiming) != cudaSuccess) {
+    delete s;
+    return set_err(BH_ERR_CUDA, "stream/event creation failed");
+  }
+  bh::set_seq_com_smem_limit();
+  *sys = s;
+  return BH_OK;
+}
+
+int bh_system_destroy(bh_system *s) {
+  if (!s) return BH_OK;
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  free_buffers(s->b);
+  if (s->side) cudaStreamDestroy(s->side);
+  if (s->side_done) cudaEventDestroy(s->side_done);
+  delete s;
+  return BH_OK;
+}
+
+int bh_system_build(bh_system *s, const double *d_m, const double *d_x, const double *d_y,
+                    const double *d_z, int64_t n, const bh_params *p, void *stream) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  int rc = check_params(p, n);
+  if (rc) return rc;
+  if (!d_m || !d_x || !d_y || !d_z) return set_err(BH_ERR_INVALID, "NULL input array");
+  BH_CUDA(cudaSetDevice(s->device));
+  s->p = *p;
+  rc = ensure_capacity(s, n);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  s->m = d_m; s->x = d_x; s->y = d_y; s->z = d_z;
+  s->n = n;
+  s->order = p->order;
+  if (n == 1) {
+    // a lone body feels no force; there is no extent to normalise by
+    BH_CUDA(cudaMemsetAsync(s->b.sc, 0, sizeof(bh::Scalars), st));
+    s->built = 1;
+    s->verify_pending = 0;
+    return BH_OK;
+  }
+  enqueue_build(s, n, 0, st);
+  BH_CUDA(cudaGetLastError());
+  s->built = 1;
+  s->verify_pending = p->strict_keys ? 1 : 0;
+  return BH_OK;
+}
+
+int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (!s->built) return set_err(BH_ERR_NOT_BUILT, "walk before build");
+  int rc = check_params(p, s->n);
+  if (rc) return rc;
+  if (p->order > s->order) return set_err(BH_ERR_INVALID, "order %d above the built order %d", p->order, s->order);
+  if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
+  BH_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t n = s->n;
+  if (n == 1) {
+    BH_CUDA(cudaMemsetAsync(d_out, 0, 3 * sizeof(double), st));
+  } else {
+    bh::WalkParams w = walk_params(p, s->order);
+    if (w.count_stats) BH_CUDA(cudaMemsetAsync(s->b.stats, 0, 4 * sizeof(unsigned long long), st));
+    if (p->precision == BH_PREC_REFERENCE)
+      bh::launch_reference_walk(n, w, s->b, d_out, nullptr, 0, nullptr, st);
+    else
+      bh::launch_walk(n, w, s->b, d_out, st);
+  }
+  if (s->verify_pending) {
+    BH_CUDA(cudaStreamWaitEvent(st, s->side_done, 0));
+    bh::launch_verify_keys(s->m, s->x, s->y, s->z, n, p->depth, s->b, st);
+    s->verify_pending = 0;
+  }
+  BH_CUDA(cudaGetLastError());
+  return BH_OK;
+}
+
+int bh_system_sync(bh_system *s, void *stream) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  BH_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (s->verify_pending && s->built) {
+    BH_CUDA(cudaStreamWaitEvent(st, s->side_done, 0));
+    bh::launch_verify_keys(s->m, s->x, s->y, s->z, s->n, s->p.depth, s->b, st);
+    s->verify_pending = 0;
+  }
+  int rc = read_scalars(s, st);
+  if (rc) return rc;
+  return status_from_device(s, 0);
+}
+
+int bh_system_forces(bh_system *s, const double *d_m, const double *d_x, const double *d_y,
+                     const double *d_z, int64_t n, const bh_params *p, double *d_out,
+                     void *stream) {
+  int rc = bh_system_build(s, d_m, d_x, d_y, d_z, n, p, stream);
+  if (rc) return rc;
+  rc = bh_system_walk(s, p, d_out, stream);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = read_scalars(s, st);
+  if (rc) return rc;
+  const bh::Scalars &h = *s->b.sc_host;
+  if (h.key_mismatch) {
+    // a key differs from the reference's: rebuild from the sequential-order
+    // centre of mass (the reference's own) and walk again
+    bh::launch_adopt_seq_com(s->b, st);
+    enqueue_build(s, n, 1, st);
+    bh_system_walk(s, p, d_out, stream);
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+  }
+  for (int attempt = 0; attempt < 4 && (s->b.sc_host->err & bh::kErrStackOverflow); ++attempt) {
+    s->stack_cap *= 2;
+    rc = ensure_capacity(s, n);
+    if (rc) return rc;
+    BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
+    rc = bh_system_walk(s, p, d_out, stream);
+    if (rc) return rc;
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+  }
+  return status_from_device(s, 0);
+}
+
+int bh_system_info(bh_system *s, int64_t *n, int *depth, int64_t *n_nodes, int64_t *n_groups,
+                   double *com4, double *ssa) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (!s->built) return set_err(BH_ERR_NOT_BUILT, "info before build");
+  BH_CUDA(cudaSetDevice(s->device));
+  int rc = read_scalars(s, 0);
+  if (rc) return rc;
+  const bh::Scalars &h = *s->b.sc_host;
+  if (n) *n = s->n;
+  if (depth) *depth = h.L;
+  if (n_nodes) *n_nodes = s->n >= 2 ? h.n_compact : 0;
+  if (n_groups) *n_groups = s->n >= 2 ? h.n_groups : 0;
+  if (com4) { com4[0] = h.com[0]; com4[1] = h.com[1]; com4[2] = h.com[2]; com4[3] = h.mass; }
+  if (ssa) *ssa = h.ssa;
+  return BH_OK;
+}
+
+int bh_system_get_keys(bh_system *s, uint64_t *keys, int32_t *perm) {
+  if (!s || !s->built) return set_err(BH_ERR_NOT_BUILT, "keys before build");
+  BH_CUDA(cudaSetDevice(s->device));
+  BH_CUDA(cudaDeviceSynchronize());
+  if (keys) BH_CUDA(cudaMemcpy(keys, s->b.k0, s->n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  if (perm) BH_CUDA(cudaMemcpy(perm, s->b.v0, s->n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return BH_OK;
+}
+
+int bh_system_get_nodes(bh_system *s, int32_t *meta4, int32_t *child8, int32_t *parent,
+                        double *com4, double *quad6, double *oct14, int32_t *level_begin) {
+  if (!s || !s->built) return set_err(BH_ERR_NOT_BUILT, "nodes before build");
+  BH_CUDA(cudaSetDevice(s->device));
+  int rc = read_scalars(s, 0);
+  if (rc) return rc;
+  const int64_t M = s->n >= 2 ? s->b.sc_host->n_compact : 0;
+  const Buffers &b = s->b;
+  if (M > 0) {
+    if (meta4) BH_CUDA(cudaMemcpy(meta4, b.cn_meta, M * sizeof(int4), cudaMemcpyDeviceToHost));
+    if (child8) BH_CUDA(cudaMemcpy(child8, b.cn_child, M * 8 * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (parent) BH_CUDA(cudaMemcpy(parent, b.cn_parent, M * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (com4) BH_CUDA(cudaMemcpy(com4, b.cn_com, M * sizeof(double4), cudaMemcpyDeviceToHost));
+    if (quad6 && s->order >= 4) BH_CUDA(cudaMemcpy(quad6, b.cn_quad, M * 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (oct14 && s->order >= 8) BH_CUDA(cudaMemcpy(oct14, b.cn_oct, M * 14 * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  if (level_begin && s->n >= 2)
+    BH_CUDA(cudaMemcpy(level_begin, b.level_begin, (s->b.sc_host->L + 2) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return BH_OK;
+}
+
+int bh_system_get_groups(bh_system *s, int32_t *group_first) {
+  if (!s || !s->built) return set_err(BH_ERR_NOT_BUILT, "groups before build");
+  BH_CUDA(cudaSetDevice(s->device));
+  int rc = read_scalars(s, 0);
+  if (rc) return rc;
+  if (s->n >= 2 && group_first)
+    BH_CUDA(cudaMemcpy(group_first, s->b.g_first, (s->b.sc_host->n_groups + 1) * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost));
+  return BH_OK;
+}
+
+int bh_system_get_stats(bh_system *s, uint64_t *stats4) {
+  if (!s || !stats4) return set_err(BH_ERR_INVALID, "NULL argument");
+  BH_CUDA(cudaSetDevice(s->device));
+  BH_CUDA(cudaDeviceSynchronize());
+  BH_CUDA(cudaMemcpy(stats4, s->b.stats, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return BH_OK;
+}
+
+int bh_system_reference_targets(bh_system *s, const bh_params *p, const int64_t *d_targets,
+                                int64_t ntargets, double *d_out, int64_t *d_counts,
+                                void *stream) {
+  if (!s || !s->built) return set_err(BH_ERR_NOT_BUILT, "reference walk before build");
+  int rc = check_params(p, s->n);
+  if (rc) return rc;
+  if (!d_targets || ntargets < 1 || !d_out) return set_err(BH_ERR_INVALID, "bad targets/output");
+  if (p->order > s->order) return set_err(BH_ERR_INVALID, "order above the built order");
+  BH_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  if (s->n == 1) {
+    BH_CUDA(cudaMemsetAsync(d_out, 0, 3 * ntargets * sizeof(double), st));
+    return BH_OK;
+  }
+  bh::WalkParams w = walk_params(p, s->order);
+  bh::launch_reference_walk(s->n, w, s->b, d_out, d_targets, ntargets, d_counts, st);
+  BH_CUDA(cudaGetLastError());
+  return BH_OK;
+}
+
+int bh_compute_forces_ex(const double *m, const double *x, const double *y, const double *z,
+                         int64_t n, const bh_params *p, double *out, void *stream) {
+  int rc = check_params(p, n);
+  if (rc) return rc;
+  if (!m || !x || !y || !z || !out) return set_err(BH_ERR_INVALID, "NULL array");
+  std::lock_guard<std::mutex> lock(g_default_mu);
+  bh_system *s = nullptr;
+  rc = default_system(&s);
+  if (rc) return rc;
+  rc = ensure_capacity(s, n);
+  if (rc) return rc;
+  rc = ensure_host_staging(s, n);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  Buffers &b = s->b;
+  BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  rc = bh_system_forces(s, b.hm, b.hx, b.hy, b.hz, n, p, b.hout, stream);
+  if (rc) return rc;
+  BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BH_CUDA(cudaStreamSynchronize(st));
+  return BH_OK;
+}
+
+int bh_compute_forces(const double *m, const double *x, const double *y, const double *z,
+                      int64_t n, double theta, double G, double eps, int order, int out_kind,
+                      double *out, void *stream) {
+  bh_params p;
+  bh_params_default(&p);
+  p.theta = theta;
+  p.G = G;
+  p.eps = eps;
+  p.order = order;
+  p.out_kind = out_kind;
+  return bh_compute_forces_ex(m, x, y, z, n, &p, out, stream);
+}
+
+int bh_compute_forces_direct(const double *m, const double *x, const double *y,
+                             const double *z, int64_t n, double G, double eps, int out_kind,
+                             double *out, void *stream) {
+  if (n < 1 || n > (int64_t)(1 << 30)) return set_err(BH_ERR_INVALID, "n out of range");
+  if (!m || !x || !y || !z || !out) return set_err(BH_ERR_INVALID, "NULL array");
+  if (out_kind != 0 && out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
+  std::lock_guard<std::mutex> lock(g_default_mu);
+  bh_system *s = nullptr;
+  int rc = default_system(&s);
+  if (rc) return rc;
+  rc = ensure_capacity(s, n);
+  if (rc) return rc;
+  rc = ensure_host_staging(s, n);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  Buffers &b = s->b;
+  BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  bh::launch_direct(b.hm, b.hx, b.hy, b.hz, n, nullptr, 0, G, eps * eps, out_kind, b.hout, st);
+  BH_CUDA(cudaGetLastError());
+  BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BH_CUDA(cudaStreamSynchronize(st));
+  return BH_OK;
+}
+
+int bh_direct_targets_device(const double *d_m, const double *d_x, const double *d_y,
+                             const double *d_z, int64_t n, const int64_t *d_targets,
+                             int64_t ntargets, double G, double eps, int out_kind, double *d_out,
+                             void *stream) {
+  if (n < 1) return set_err(BH_ERR_INVALID, "n must be >= 1");
+  if (!d_m || !d_x || !d_y || !d_z || !d_out) return set_err(BH_ERR_INVALID, "NULL array");
+  if (d_targets && ntargets < 1) return set_err(BH_ERR_INVALID, "ntargets must be >= 1");
+  if (out_kind != 0 && out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
+  bh::launch_direct(d_m, d_x, d_y, d_z, n, d_targets, ntargets, G, eps * eps, out_kind, d_out,
+                    (cudaStream_t)stream);
+  BH_CUDA(cudaGetLastError());
+  return BH_OK;
+}
+
+int bh_probe_fma_peak(int device, double *gflops2) {
+  if (!gflops2) return set_err(BH_ERR_INVALID, "NULL output");
+  BH_CUDA(cudaSetDevice(device));
+  if (bh::probe_fma(gflops2)) return set_err(BH_ERR_CUDA, "probe failed");
+  return BH_OK;
+}
+
+}  // extern "C"

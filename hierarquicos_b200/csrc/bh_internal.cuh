@@ -1,0 +1,150 @@
+// Internal declarations shared by the CUDA translation units of the
+// Barnes-Hut force engine.  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/hierarquicos_bh.h"
+
+namespace bh {
+
+constexpr int kWarp = 32;
+
+__host__ __device__ __forceinline__ int64_t bh_min64(int64_t a, int64_t b) { return a < b ? a : b; }
+constexpr int kMaxDepth = 21;          // 3 * 21 = 63 key bits
+constexpr int kNumLevels = kMaxDepth + 2;  // level_begin has L + 2 entries
+
+// Error bits collected on the device and returned as status codes.
+enum DeviceError : int {
+  kErrNone = 0,
+  kErrNonFinite = 1 << 0,      // NaN / Inf position or mass, or zero total mass
+  kErrStackOverflow = 1 << 1,  // walk stack capacity exceeded
+  kErrIndex = 1 << 2,          // internal index out of range (a bug)
+  kErrDuplicates = 1 << 3,     // automatic depth impossible: coincident bodies
+  kErrChildren = 1 << 4,       // more than 8 children (a bug)
+};
+
+// Scalars computed on the device for one system.  Plain doubles so that the
+// host can read them back with a single copy.
+struct Scalars {
+  double bmin[3], bmax[3];  // bounding box of the positions
+  double com[3], mass;      // centre of mass used for the keys
+  double com_seq[3], mass_seq;  // centre of mass in the reference's order
+  double ssa;               // side of the root cube, amp * largest extent
+  double vcen[3];           // centre of the normalised box (keys)
+  double vcen_seq[3];
+  int L;                    // key depth actually used
+  int n_compact;            // number of compact internal nodes
+  int n_groups;             // number of target groups
+  int err;                  // DeviceError bits
+  int key_mismatch;         // keys differ from the sequential-COM keys
+  int max_lcp;              // deepest shared octal prefix (auto depth)
+  int pad[2];
+};
+
+// Per-system device buffers.  Sized for `cap` particles.
+struct Buffers {
+  int64_t cap = 0;
+  // inputs staged from the host (host-pointer API only)
+  double *hm = nullptr, *hx = nullptr, *hy = nullptr, *hz = nullptr;
+  double *hout = nullptr;
+  // keys and sort
+  uint64_t *k0 = nullptr, *k1 = nullptr;
+  int32_t *v0 = nullptr, *v1 = nullptr;
+  int32_t *hist = nullptr;
+  int64_t hist_cap = 0;
+  double *partials = nullptr;
+  // sorted particles (x, y, z, m)
+  double4 *spos = nullptr;
+  // binary radix tree over the sorted keys (n - 1 internal nodes)
+  int32_t *bn_left = nullptr, *bn_right = nullptr, *bn_parent = nullptr;
+  int32_t *bn_first = nullptr, *bn_last = nullptr, *bn_level = nullptr;
+  int32_t *bn_flag = nullptr, *bin2cn = nullptr;
+  // compact octree, ordered by (level, first particle)
+  int32_t *cn_bin = nullptr;
+  int4 *cn_meta = nullptr;       // first, count, level, nchild
+  int32_t *cn_child = nullptr;   // 8 per node; >= 0 node, < 0 particle ~p
+  int32_t *cn_parent = nullptr;
+  double4 *cn_com = nullptr;     // com x, y, z, mass
+  double *cn_quad = nullptr;     // 6 per node: xx yy zz xy xz yz
+  double *cn_oct = nullptr;      // 14 per node (octree_default.f90 layout)
+  float4 *cn_fq = nullptr;       // 2 per node, normalised FP32 quadrupole + trace
+  float4 *cn_fo = nullptr;       // 4 per node, normalised FP32 octupole
+  int32_t *level_begin = nullptr;  // kNumLevels + 1 entries
+  // target groups
+  int32_t *gflag = nullptr, *gscan = nullptr, *g_first = nullptr;
+  int32_t *inv_perm = nullptr;
+  // scan scratch
+  int32_t *scan_tmp = nullptr;
+  int64_t scan_tmp_cap = 0;
+  // walk
+  int32_t *wstack = nullptr;
+  int64_t wstack_cap = 0;   // entries per warp slot
+  int64_t wstack_slots = 0;
+  int32_t *counters = nullptr;   // [0] group cursor
+  unsigned long long *stats = nullptr;  // interaction counters
+  Scalars *sc = nullptr;
+  Scalars *sc_host = nullptr;    // pinned mirror
+};
+
+// ---- kernels / launchers (one translation unit each) ----
+
+// keys: bbox + COM + keys.  com_mode: 0 separate multiply and add, 1 fused.
+void launch_keys(const double *m, const double *x, const double *y, const double *z, int64_t n,
+                 int L, double amp, int com_mode, int strict, Buffers &b, cudaStream_t s,
+                 cudaStream_t side, cudaEvent_t side_done);
+void launch_verify_keys(const double *m, const double *x, const double *y, const double *z,
+                        int64_t n, int L, Buffers &b, cudaStream_t s);
+void launch_auto_depth(int64_t n, Buffers &b, cudaStream_t s);
+void launch_adopt_seq_com(Buffers &b, cudaStream_t s);
+void launch_keys_only(const double *x, const double *y, const double *z, int64_t n, int L,
+                      Buffers &b, cudaStream_t s);
+void set_seq_com_smem_limit();
+inline int grid_for(int64_t n, int threads, int cap) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// stable LSD radix sort of (key, value) pairs over bits [0, bits); the
+// result ends in (k0, v0).  n_dev, when given, holds the element count on the
+// device (n is then an upper bound).
+void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
+                      const int32_t *n_dev, int bits, int32_t *hist, cudaStream_t s);
+int64_t radix_hist_entries(int64_t n);
+
+// exclusive scan of n int32 values; total written to *total (device) if given
+void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
+                    int32_t *total, int32_t *tmp, cudaStream_t s);
+int64_t scan_tmp_entries(int64_t n);
+
+void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
+                   Buffers &b, cudaStream_t s);
+void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s);
+void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s);
+void launch_groups(int64_t n, int group_size, Buffers &b, cudaStream_t s);
+
+struct WalkParams {
+  double theta2, G, eps2;
+  int order;       // 1, 4, 8
+  int out_kind;    // 0 forces, 1 accelerations
+  int precision;   // BH_PREC_*
+  int group_size;  // 32 or 64
+  int leaf_cap;
+  int count_stats;
+};
+// Returns the number of warp slots used (for stack sizing).
+void launch_walk(int64_t n, const WalkParams &p, Buffers &b, double *out, cudaStream_t s);
+void launch_reference_walk(int64_t n, const WalkParams &p, Buffers &b, double *out,
+                           const int64_t *targets, int64_t ntargets, int64_t *counts,
+                           cudaStream_t s);
+int64_t walk_slots();
+int probe_fma(double *gflops2);
+
+void launch_direct(const double *m, const double *x, const double *y, const double *z, int64_t n,
+                   const int64_t *targets, int64_t ntargets, double G, double eps2, int out_kind,
+                   double *out, cudaStream_t s);
+
+}  // namespace bh

@@ -1,0 +1,347 @@
+// Bounding box, centre of mass, normalisation and 63-bit Morton keys.
+//
+// Follows fortran/morton/morton_octree.f90:359-395 (generate_nodes steps 1-5)
+// and :184-213 (morton_key).  All arithmetic that feeds a key uses explicitly
+// rounded intrinsics so that no multiply-add is contracted and every key is
+// bit-identical to the reference's for the same centre of mass.
+//
+// The reference sums the centre of mass sequentially (:364-370).  A parallel
+// sum may differ in the last bits, and keys depend on those bits only for a
+// body that sits within an ulp of a 2^-21 cell boundary.  The pipeline
+// therefore computes keys from a deterministic parallel sum, and, when strict
+// keys are requested, a side stream recomputes the sum in the reference's
+// order on one thread block; launch_verify_keys then recomputes every key with
+// that centre of mass and flags any difference, in which case the host
+// rebuilds with the sequential centre of mass (see bh_abi.cu).
+#include <math.h>
+
+#include "bh_internal.cuh"
+
+namespace bh {
+
+namespace {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs; fixed so the sum order is fixed
+
+// 21-bit coordinate -> 63-bit interleave, x in the most significant slot of
+// each octal digit (morton_octree.f90:205-212).
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+  v &= 0x1fffffull;
+  v = (v | (v << 32)) & 0x1f00000000ffffull;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__device__ __forceinline__ int64_t quantise(double xn, int L) {
+  // FLOOR(x * 2^L) clamped to 2^L - 1; x * 2^L is exact.
+  const double scale = (double)(1ll << L);
+  double f = floor(__dmul_rn(xn, scale));
+  int64_t i = (int64_t)f;
+  int64_t top = (1ll << L) - 1;
+  if (i > top) i = top;
+  if (i < 0) i = 0;
+  return i;
+}
+
+__device__ __forceinline__ uint64_t key_of(double x, double y, double z, const double com[3],
+                                           double ssa, const double vcen[3], int L, int *bad) {
+  // positions_norm = (q - qcm) / ssa, then + 0.5 - ssi (morton_octree.f90:373-384)
+  double vx = __ddiv_rn(__dsub_rn(x, com[0]), ssa);
+  double vy = __ddiv_rn(__dsub_rn(y, com[1]), ssa);
+  double vz = __ddiv_rn(__dsub_rn(z, com[2]), ssa);
+  double xn = __dsub_rn(__dadd_rn(vx, 0.5), vcen[0]);
+  double yn = __dsub_rn(__dadd_rn(vy, 0.5), vcen[1]);
+  double zn = __dsub_rn(__dadd_rn(vz, 0.5), vcen[2]);
+  if (!(xn >= 0.0 && xn < 1.0 && yn >= 0.0 && yn < 1.0 && zn >= 0.0 && zn < 1.0)) *bad = 1;
+  uint64_t ix = (uint64_t)quantise(xn, L), iy = (uint64_t)quantise(yn, L),
+           iz = (uint64_t)quantise(zn, L);
+  return (spread3(ix) << 2) | (spread3(iy) << 1) | spread3(iz);
+}
+
+// Partial reductions: min/max per axis, sum m, sum m x, sum m y, sum m z.
+// Fixed grid and fixed tree order: the result is deterministic.
+__global__ void __launch_bounds__(kRedThreads)
+reduce_partials(const double *__restrict__ m, const double *__restrict__ x,
+                const double *__restrict__ y, const double *__restrict__ z, int64_t n,
+                int com_mode, double *__restrict__ partials) {
+  __shared__ double s[10][kRedThreads];
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double sm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    double a = x[p], b = y[p], c = z[p], w = m[p];
+    mn[0] = fmin(mn[0], a); mx[0] = fmax(mx[0], a);
+    mn[1] = fmin(mn[1], b); mx[1] = fmax(mx[1], b);
+    mn[2] = fmin(mn[2], c); mx[2] = fmax(mx[2], c);
+    sm = __dadd_rn(sm, w);
+    if (com_mode) {
+      sx = __fma_rn(w, a, sx); sy = __fma_rn(w, b, sy); sz = __fma_rn(w, c, sz);
+    } else {
+      sx = __dadd_rn(sx, __dmul_rn(w, a));
+      sy = __dadd_rn(sy, __dmul_rn(w, b));
+      sz = __dadd_rn(sz, __dmul_rn(w, c));
+    }
+    // NaN check folded into the sums (propagates)
+  }
+  int t = threadIdx.x;
+  s[0][t] = mn[0]; s[1][t] = mn[1]; s[2][t] = mn[2];
+  s[3][t] = mx[0]; s[4][t] = mx[1]; s[5][t] = mx[2];
+  s[6][t] = sm; s[7][t] = sx; s[8][t] = sy; s[9][t] = sz;
+  __syncthreads();
+  for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+    if (t < w) {
+      for (int k = 0; k < 3; ++k) s[k][t] = fmin(s[k][t], s[k][t + w]);
+      for (int k = 3; k < 6; ++k) s[k][t] = fmax(s[k][t], s[k][t + w]);
+      for (int k = 6; k < 10; ++k) s[k][t] = __dadd_rn(s[k][t], s[k][t + w]);
+    }
+    __syncthreads();
+  }
+  if (t < 10) partials[blockIdx.x * 10 + t] = s[t][0];
+}
+
+__device__ void finalize_norm(Scalars *sc, const double com[3], double vcen[3]) {
+  // normalised box centre: min/max of fl(fl(q - com) / ssa) are the images of
+  // the coordinate min/max because rounding is monotonic.
+  for (int k = 0; k < 3; ++k) {
+    double vmin = __ddiv_rn(__dsub_rn(sc->bmin[k], com[k]), sc->ssa);
+    double vmax = __ddiv_rn(__dsub_rn(sc->bmax[k], com[k]), sc->ssa);
+    vcen[k] = __dmul_rn(0.5, __dadd_rn(vmin, vmax));
+  }
+}
+
+__global__ void finalize_kernel(const double *__restrict__ partials, int nparts, double amp,
+                                int L, Scalars *sc) {
+  if (threadIdx.x != 0) return;
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  double sm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int b = 0; b < nparts; ++b) {
+    const double *q = partials + 10 * b;
+    for (int k = 0; k < 3; ++k) { mn[k] = fmin(mn[k], q[k]); mx[k] = fmax(mx[k], q[3 + k]); }
+    sm = __dadd_rn(sm, q[6]);
+    sx = __dadd_rn(sx, q[7]); sy = __dadd_rn(sy, q[8]); sz = __dadd_rn(sz, q[9]);
+  }
+  for (int k = 0; k < 3; ++k) { sc->bmin[k] = mn[k]; sc->bmax[k] = mx[k]; }
+  double ext = __dsub_rn(mx[0], mn[0]);
+  double ey = __dsub_rn(mx[1], mn[1]), ez = __dsub_rn(mx[2], mn[2]);
+  if (ey > ext) ext = ey;
+  if (ez > ext) ext = ez;
+  sc->ssa = __dmul_rn(amp, ext);
+  sc->mass = sm;
+  sc->com[0] = __ddiv_rn(sx, sm);
+  sc->com[1] = __ddiv_rn(sy, sm);
+  sc->com[2] = __ddiv_rn(sz, sm);
+  sc->L = L;
+  sc->err = 0;
+  sc->key_mismatch = 0;
+  bool ok = isfinite(sm) && sm > 0.0 && isfinite(sc->com[0]) && isfinite(sc->com[1]) &&
+            isfinite(sc->com[2]) && isfinite(ext) && ext > 0.0;
+  if (!ok) sc->err |= kErrNonFinite;
+  finalize_norm(sc, sc->com, sc->vcen);
+}
+
+__global__ void __launch_bounds__(256)
+keys_kernel(const double *__restrict__ x, const double *__restrict__ y,
+            const double *__restrict__ z, int64_t n, int L, const Scalars *__restrict__ sc,
+            uint64_t *__restrict__ keys, int32_t *__restrict__ vals, int *err) {
+  const double com[3] = {sc->com[0], sc->com[1], sc->com[2]};
+  const double vcen[3] = {sc->vcen[0], sc->vcen[1], sc->vcen[2]};
+  const double ssa = sc->ssa;
+  int bad = 0;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = key_of(x[p], y[p], z[p], com, ssa, vcen, kMaxDepth, &bad);
+    keys[p] = (L == kMaxDepth || L == 0) ? k : (k >> (3 * (kMaxDepth - L)));
+    vals[p] = (int32_t)p;
+  }
+  if (bad) atomicOr(err, kErrNonFinite);
+}
+
+// Sequential centre of mass in the reference's order (morton_octree.f90:364-370):
+// qcm = qcm + m_p q_p, mass = mass + m_p for p = 1..N.  Warps 1..7 stage the
+// next tile into shared memory while warp 0 folds the current tile; all lanes
+// of warp 0 run the same chain (broadcast reads), so there is no divergence.
+constexpr int kSeqTile = 1024;
+constexpr int kSeqThreads = 256;
+
+__global__ void __launch_bounds__(kSeqThreads)
+seq_com_kernel(const double *__restrict__ m, const double *__restrict__ x,
+               const double *__restrict__ y, const double *__restrict__ z, int64_t n,
+               int com_mode, Scalars *sc) {
+  extern __shared__ double4 tile[];  // 2 x kSeqTile entries: (m, x, y, z)
+  const int warp = threadIdx.x / kWarp;
+  const int64_t ntiles = (n + kSeqTile - 1) / kSeqTile;
+  double ax = 0.0, ay = 0.0, az = 0.0, am = 0.0;
+  auto stage = [&](int64_t t, int buf) {
+    if (warp == 0) return;
+    for (int i = threadIdx.x - kWarp; i < kSeqTile; i += kSeqThreads - kWarp) {
+      int64_t p = t * kSeqTile + i;
+      double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (p < n) v = make_double4(m[p], x[p], y[p], z[p]);
+      tile[buf * kSeqTile + i] = v;
+    }
+  };
+  stage(0, 0);
+  __syncthreads();
+  for (int64_t t = 0; t < ntiles; ++t) {
+    int buf = (int)(t & 1);
+    if (t + 1 < ntiles) stage(t + 1, buf ^ 1);
+    if (warp == 0) {
+      int cnt = (int)bh_min64(kSeqTile, n - t * kSeqTile);
+      const double4 *q = tile + buf * kSeqTile;
+      if (com_mode) {
+#pragma unroll 8
+        for (int i = 0; i < cnt; ++i) {
+          double4 v = q[i];
+          ax = __fma_rn(v.x, v.y, ax);
+          ay = __fma_rn(v.x, v.z, ay);
+          az = __fma_rn(v.x, v.w, az);
+          am = __dadd_rn(am, v.x);
+        }
+      } else {
+#pragma unroll 8
+        for (int i = 0; i < cnt; ++i) {
+          double4 v = q[i];
+          ax = __dadd_rn(ax, __dmul_rn(v.x, v.y));
+          ay = __dadd_rn(ay, __dmul_rn(v.x, v.z));
+          az = __dadd_rn(az, __dmul_rn(v.x, v.w));
+          am = __dadd_rn(am, v.x);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    sc->mass_seq = am;
+    sc->com_seq[0] = __ddiv_rn(ax, am);
+    sc->com_seq[1] = __ddiv_rn(ay, am);
+    sc->com_seq[2] = __ddiv_rn(az, am);
+  }
+}
+
+// Recomputes every key with the sequential-order centre of mass and compares
+// it with the key the tree was built from (sorted position i holds original
+// particle perm[i]).
+__global__ void __launch_bounds__(256)
+verify_keys_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                   const double *__restrict__ z, int64_t n, Scalars *sc,
+                   const uint64_t *__restrict__ skeys, const int32_t *__restrict__ perm) {
+  // identical centre of mass: nothing can differ
+  if (sc->com_seq[0] == sc->com[0] && sc->com_seq[1] == sc->com[1] &&
+      sc->com_seq[2] == sc->com[2])
+    return;
+  double vcen[3];
+  for (int k = 0; k < 3; ++k) {
+    double vmin = __ddiv_rn(__dsub_rn(sc->bmin[k], sc->com_seq[k]), sc->ssa);
+    double vmax = __ddiv_rn(__dsub_rn(sc->bmax[k], sc->com_seq[k]), sc->ssa);
+    vcen[k] = __dmul_rn(0.5, __dadd_rn(vmin, vmax));
+  }
+  const double com[3] = {sc->com_seq[0], sc->com_seq[1], sc->com_seq[2]};
+  const int L = sc->L;
+  int bad = 0, diff = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int32_t p = perm[i];
+    uint64_t k = key_of(x[p], y[p], z[p], com, sc->ssa, vcen, kMaxDepth, &bad);
+    if (L != kMaxDepth) k >>= 3 * (kMaxDepth - L);
+    if (k != skeys[i]) diff = 1;
+  }
+  if (diff) atomicExch(&sc->key_mismatch, 1);
+}
+
+// Copies the sequential centre of mass over the speculative one (used by the
+// rebuild after a mismatch) and recomputes the normalisation centre.
+__global__ void adopt_seq_com_kernel(Scalars *sc) {
+  if (threadIdx.x != 0) return;
+  sc->com[0] = sc->com_seq[0];
+  sc->com[1] = sc->com_seq[1];
+  sc->com[2] = sc->com_seq[2];
+  sc->mass = sc->mass_seq;
+  finalize_norm(sc, sc->com, sc->vcen);
+}
+
+// Smallest depth with unique keys (choose_depth, morton_octree.f90:217-244):
+// keys at depth L are the 21-level keys shifted right, so depth L separates
+// every pair iff L exceeds the deepest common octal prefix of sorted
+// neighbours.
+__global__ void max_lcp_kernel(const uint64_t *__restrict__ k, int64_t n, Scalars *sc) {
+  int best = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t d = k[i] ^ k[i - 1];
+    int lcp = d ? (__clzll(d) - 1) / 3 : kMaxDepth;
+    best = max(best, lcp);
+  }
+  atomicMax(&sc->max_lcp, best);
+}
+
+__global__ void apply_depth_kernel(uint64_t *__restrict__ k, int64_t n, Scalars *sc) {
+  int L = sc->max_lcp + 1;
+  if (sc->max_lcp >= kMaxDepth) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      sc->err |= kErrDuplicates;
+      sc->L = kMaxDepth;
+    }
+    return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) sc->L = L;
+  int shift = 3 * (kMaxDepth - L);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    k[i] >>= shift;
+}
+
+}  // namespace
+
+void launch_keys(const double *m, const double *x, const double *y, const double *z, int64_t n,
+                 int L, double amp, int com_mode, int strict, Buffers &b, cudaStream_t s,
+                 cudaStream_t side, cudaEvent_t side_done) {
+  reduce_partials<<<kRedBlocks, kRedThreads, 0, s>>>(m, x, y, z, n, com_mode, b.partials);
+  finalize_kernel<<<1, 32, 0, s>>>(b.partials, kRedBlocks, amp, L == 0 ? kMaxDepth : L, b.sc);
+  if (strict && side) {
+    // the side stream must see the inputs: it is ordered after everything
+    // already queued on s by the caller through an event recorded there
+    cudaEvent_t ready;
+    cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    cudaEventRecord(ready, s);
+    cudaStreamWaitEvent(side, ready, 0);
+    cudaEventDestroy(ready);
+    size_t smem = 2 * kSeqTile * sizeof(double4);
+    seq_com_kernel<<<1, kSeqThreads, smem, side>>>(m, x, y, z, n, com_mode, b.sc);
+    cudaEventRecord(side_done, side);
+  }
+  keys_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(x, y, z, n, L == 0 ? kMaxDepth : L, b.sc,
+                                                         b.k0, b.v0, &b.sc->err);
+}
+
+// Keys from the centre of mass already in the scalars (rebuild path).
+void launch_keys_only(const double *x, const double *y, const double *z, int64_t n, int L,
+                      Buffers &b, cudaStream_t s) {
+  keys_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(x, y, z, n, L == 0 ? kMaxDepth : L, b.sc,
+                                                         b.k0, b.v0, &b.sc->err);
+}
+
+void launch_auto_depth(int64_t n, Buffers &b, cudaStream_t s) {
+  cudaMemsetAsync(&b.sc->max_lcp, 0, sizeof(int), s);
+  max_lcp_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(b.k0, n, b.sc);
+  apply_depth_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(b.k0, n, b.sc);
+}
+
+void launch_verify_keys(const double *m, const double *x, const double *y, const double *z,
+                        int64_t n, int L, Buffers &b, cudaStream_t s) {
+  (void)m;
+  (void)L;
+  verify_keys_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(x, y, z, n, b.sc, b.k0, b.v0);
+}
+
+void launch_adopt_seq_com(Buffers &b, cudaStream_t s) { adopt_seq_com_kernel<<<1, 32, 0, s>>>(b.sc); }
+
+void set_seq_com_smem_limit() {
+  cudaFuncSetAttribute(seq_com_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(2 * kSeqTile * sizeof(double4)));
+}
+
+}  // namespace bh

@@ -1,0 +1,686 @@
+// Tree walks.
+//
+// 1. Group walk (the production path), after Barnes (1990) as restated by
+//    fortran/octree_default.f90:1811-2095 (forces_groups / group_worker): one
+//    warp per group of <= 64 Morton-contiguous targets.  The warp walks the
+//    tree 32 nodes at a time from a per-warp stack, tests each node with the
+//    box-distance MAC of :1927-1936 (size^2 <= theta^2 * dist^2 from the
+//    node's centre of mass to the group's bounding box), queues accepted
+//    nodes as cells and the bodies of opened leaves / lone particles as
+//    bodies, and evaluates the queues in batches of 32: lane j stages entry j
+//    (a coalesced load) into shared memory and every lane then sweeps the 32
+//    staged entries (broadcast reads) for its own 1 or 2 targets.  Each batch
+//    is summed in registers and Kahan-added (Kahan 1965) into the per-target
+//    accumulator.  Positions are taken relative to the group's centre in FP64
+//    and only then rounded, and everything is scaled to the root cube side and
+//    total mass, so the FP32 arithmetic sees O(1) numbers.  The cell formulas
+//    are the reference's (:1993-2083) with r^-3 factored out so that no
+//    intermediate power of r overflows FP32.
+//    Because the box distance never exceeds a member's own distance, every
+//    accepted cell also passes the per-target MAC of the classic walk.
+//
+// 2. Reference walk: one thread per target with the semantics of
+//    fortran/morton/morton_octree.f90:627-766 (barnes_hut) in FP64 over the
+//    compact tree: the node containing the target is always opened, cells are
+//    tested with the target-to-centre distance, lone particles are monopoles
+//    at m*q/m, level-L leaves are summed particle by particle.  Used to check
+//    the tree against the reference and to count the reference's interactions.
+#include <math.h>
+
+#include "bh_internal.cuh"
+
+namespace bh {
+
+namespace {
+
+constexpr int kWalkWarps = 4;
+constexpr int kCellQ = 64;
+constexpr int kBodyPerLane = 16;
+constexpr int kBodyQ = 32 + kWarp * kBodyPerLane;  // 544
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename T> struct Ops;
+template <> struct Ops<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float rsq(float r2) { return r2 > 0.0f ? rsqrtf(r2) : 0.0f; }
+};
+template <> struct Ops<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double rsq(double r2) { return r2 > 0.0 ? rsqrt(r2) : 0.0; }
+};
+
+template <typename T>
+__device__ __forceinline__ void kahan_add(T &s, T &c, T x) {
+  T y = Ops<T>::sub(x, c);
+  T t = Ops<T>::add(s, y);
+  c = Ops<T>::sub(Ops<T>::sub(t, s), y);
+  s = t;
+}
+
+template <int ORDER> struct StageWords { static constexpr int value = ORDER >= 8 ? 24 : (ORDER >= 4 ? 12 : 4); };
+
+template <typename T, int ORDER>
+struct __align__(16) WarpSmem {
+  T stage[kWarp * StageWords<ORDER>::value];
+  int cellq[kCellQ];
+  int bodyq[kBodyQ];
+};
+
+struct WalkArgs {
+  const int4 *meta;
+  const int32_t *child;
+  const double4 *com;
+  const double *quad;
+  const double *oct;
+  const float4 *fq;
+  const float4 *fo;
+  const double4 *spos;
+  const int32_t *perm;
+  const int32_t *g_first;
+  Scalars *sc;
+  int32_t *cursor;
+  int32_t *stack;
+  int64_t stack_cap;
+  unsigned long long *stats;
+  double *out;
+  int64_t n;
+  double theta2, G, eps2;
+  int out_kind, leaf_cap, count_stats;
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    int t = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += t;
+  }
+  total = __shfl_sync(kFull, x, kWarp - 1);
+  return x - v;
+}
+
+// Stage one cell (node j) as T words: rel x, y, z, mass, then quadrupole
+// (xx yy zz xy xz yz tr), then octupole (O1..O10, O12, O13, O14).
+template <typename T, int ORDER>
+__device__ __forceinline__ void stage_cell(T *w, int j, const WalkArgs &a, const double gc[3],
+                                           double inv_s, double inv_m, double nq, double no) {
+  const double4 c = a.com[j];
+  w[0] = (T)((c.x - gc[0]) * inv_s);
+  w[1] = (T)((c.y - gc[1]) * inv_s);
+  w[2] = (T)((c.z - gc[2]) * inv_s);
+  w[3] = (T)(c.w * inv_m);
+  if (ORDER >= 4) {
+    if (sizeof(T) == 4) {
+      const float4 q0 = a.fq[2 * (int64_t)j], q1 = a.fq[2 * (int64_t)j + 1];
+      w[4] = (T)q0.x; w[5] = (T)q0.y; w[6] = (T)q0.z; w[7] = (T)q0.w;
+      w[8] = (T)q1.x; w[9] = (T)q1.y; w[10] = (T)q1.z;
+    } else {
+      const double *q = a.quad + 6 * (int64_t)j;
+      double q0 = q[0] * nq, q1 = q[1] * nq, q2 = q[2] * nq;
+      w[4] = (T)q0; w[5] = (T)q1; w[6] = (T)q2;
+      w[7] = (T)(q[3] * nq); w[8] = (T)(q[4] * nq); w[9] = (T)(q[5] * nq);
+      w[10] = (T)(q0 + q1 + q2);
+    }
+  }
+  if (ORDER >= 8) {
+    if (sizeof(T) == 4) {
+      const float4 *f = a.fo + 4 * (int64_t)j;
+      float4 o0 = f[0], o1 = f[1], o2 = f[2], o3 = f[3];
+      w[12] = (T)o0.x; w[13] = (T)o0.y; w[14] = (T)o0.z; w[15] = (T)o0.w;
+      w[16] = (T)o1.x; w[17] = (T)o1.y; w[18] = (T)o1.z; w[19] = (T)o1.w;
+      w[20] = (T)o2.x; w[21] = (T)o2.y; w[22] = (T)o2.z; w[23] = (T)o2.w;
+      w[11] = (T)o3.x;
+    } else {
+      const double *o = a.oct + 14 * (int64_t)j;
+      for (int k = 0; k < 10; ++k) w[12 + k] = (T)(o[k] * no);
+      w[22] = (T)(o[11] * no);
+      w[23] = (T)(o[12] * no);
+      w[11] = (T)(o[13] * no);
+    }
+  }
+}
+
+// One cell interaction, accumulated into (bx, by, bz); returns nothing.
+// r^-3 is factored out of every term (see file comment).
+template <typename T, int ORDER>
+__device__ __forceinline__ void cell_force(const T *w, T rx, T ry, T rz, T eps2, T &bx, T &by,
+                                           T &bz) {
+  const T dx = w[0] - rx, dy = w[1] - ry, dz = w[2] - rz;
+  const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+  const T rinv = Ops<T>::rsq(r2);
+  const T r2i = rinv * rinv;
+  const T r3i = rinv * r2i;
+  if (ORDER < 4) {
+    const T f = w[3] * r3i;
+    bx = fma(f, dx, bx); by = fma(f, dy, by); bz = fma(f, dz, bz);
+    return;
+  }
+  const T qxx = w[4], qyy = w[5], qzz = w[6], qxy = w[7], qxz = w[8], qyz = w[9], tr = w[10];
+  const T qx = fma(qxx, dx, fma(qxy, dy, qxz * dz));
+  const T qy = fma(qxy, dx, fma(qyy, dy, qyz * dz));
+  const T qz = fma(qxz, dx, fma(qyz, dy, qzz * dz));
+  const T dqd = fma(dx, qx, fma(dy, qy, dz * qz));
+  // r^3 s = M - 1.5 tr r^-2 + 7.5 dQd r^-4
+  const T A = fma((T)7.5 * dqd, r2i * r2i, fma((T)-1.5 * tr, r2i, w[3]));
+  const T m3 = (T)-3.0 * r2i;
+  T fx = fma(A, dx, m3 * qx), fy = fma(A, dy, m3 * qy), fz = fma(A, dz, m3 * qz);
+  if (ORDER >= 8) {
+    const T O1 = w[12], O2 = w[13], O3 = w[14], O4 = w[15], O5 = w[16], O6 = w[17], O7 = w[18],
+            O8 = w[19], O9 = w[20], O10 = w[21], O12 = w[22], O13 = w[23], O14 = w[11];
+    const T s7 = (T)7.5 * r2i * r2i;   // 7.5 r^-4
+    const T s5 = (T)-1.5 * r2i;        // -1.5 r^-2
+    const T s9 = (T)-17.5 * r2i * r2i * r2i;  // -17.5 r^-6
+    const T xx = dx * dx, yy = dy * dy, zz = dz * dz, xy = dx * dy, xz = dx * dz, yz = dy * dz;
+    const T oc = s7 * fma(dx, O12, fma(dy, O13, dz * O14));
+    T ox = fma(s5, O12, dx * oc), oy = fma(s5, O13, dy * oc), oz = fma(s5, O14, dz * oc);
+    ox = fma(s7, fma(xx, O1, fma(yy, O2, zz * O3)) + (T)2 * fma(xy, O4, fma(xz, O7, yz * O10)), ox);
+    oy = fma(s7, fma(xx, O4, fma(yy, O5, zz * O6)) + (T)2 * fma(xy, O2, fma(xz, O10, yz * O8)), oy);
+    oz = fma(s7, fma(xx, O7, fma(yy, O8, zz * O9)) + (T)2 * fma(xy, O10, fma(xz, O3, yz * O6)), oz);
+    T c3 = fma(xx * dx, O1, fma(yy * dy, O5, zz * dz * O9));
+    c3 = fma((T)3, fma(xx * dy, O4, fma(xx * dz, O7, xy * dy * O2)), c3);
+    c3 = fma((T)3, fma(yy * dz, O8, fma(xz * dz, O3, yz * dz * O6)), c3);
+    c3 = fma((T)6 * xy, dz * O10, c3);
+    c3 = s9 * c3;
+    fx += fma(dx, c3, ox); fy += fma(dy, c3, oy); fz += fma(dz, c3, oz);
+  }
+  bx = fma(r3i, fx, bx); by = fma(r3i, fy, by); bz = fma(r3i, fz, bz);
+}
+
+template <typename T, int ORDER, int TPL>
+__global__ void __launch_bounds__(kWalkWarps * kWarp)
+group_walk_kernel(WalkArgs a) {
+  __shared__ WarpSmem<T, ORDER> shm[kWalkWarps];
+  constexpr int W = StageWords<ORDER>::value;
+  constexpr bool kKahan = sizeof(T) == 4;
+  const int lane = threadIdx.x & (kWarp - 1), wid = threadIdx.x / kWarp;
+  WarpSmem<T, ORDER> &S = shm[wid];
+  const int64_t slot = (int64_t)blockIdx.x * kWalkWarps + wid;
+  int32_t *stack = a.stack + slot * a.stack_cap;
+  const int stack_cap = (int)a.stack_cap;
+  const int ngroups = a.sc->n_groups;
+  const double ssa = a.sc->ssa, Mtot = a.sc->mass;
+  const double inv_s = 1.0 / ssa, inv_m = 1.0 / Mtot;
+  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
+  const T eps2 = (T)(a.eps2 * inv_s * inv_s);
+  const T theta2 = (T)a.theta2;
+  const unsigned lt = (1u << lane) - 1u;
+  int err = 0;
+  unsigned long long n_pp = 0, n_pc = 0, n_tests = 0;
+
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(a.cursor, 1);
+    g = __shfl_sync(kFull, g, 0);
+    if (g >= ngroups) break;
+    const int gf = a.g_first[g];
+    const int gn = a.g_first[g + 1] - gf;
+
+    double px[TPL], py[TPL], pz[TPL];
+    bool valid[TPL];
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) {
+      const int k = lane + kWarp * t;
+      valid[t] = k < gn;
+      const double4 p = a.spos[gf + (valid[t] ? k : 0)];
+      px[t] = p.x; py[t] = p.y; pz[t] = p.z;
+    }
+    double lo[3] = {px[0], py[0], pz[0]}, hi[3] = {px[0], py[0], pz[0]};
+#pragma unroll
+    for (int t = 1; t < TPL; ++t) {
+      lo[0] = fmin(lo[0], px[t]); hi[0] = fmax(hi[0], px[t]);
+      lo[1] = fmin(lo[1], py[t]); hi[1] = fmax(hi[1], py[t]);
+      lo[2] = fmin(lo[2], pz[t]); hi[2] = fmax(hi[2], pz[t]);
+    }
+    double gc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) gc[k] = 0.5 * (warp_min(lo[k]) + warp_max(hi[k]));
+    T rx[TPL], ry[TPL], rz[TPL];
+    T ax[TPL], ay[TPL], az[TPL], cx[TPL], cy[TPL], cz[TPL];
+    T blo[3], bhi[3];
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) {
+      rx[t] = (T)((px[t] - gc[0]) * inv_s);
+      ry[t] = (T)((py[t] - gc[1]) * inv_s);
+      rz[t] = (T)((pz[t] - gc[2]) * inv_s);
+      ax[t] = ay[t] = az[t] = cx[t] = cy[t] = cz[t] = (T)0;
+      if (t == 0) { blo[0] = bhi[0] = rx[0]; blo[1] = bhi[1] = ry[0]; blo[2] = bhi[2] = rz[0]; }
+      else {
+        blo[0] = min(blo[0], rx[t]); bhi[0] = max(bhi[0], rx[t]);
+        blo[1] = min(blo[1], ry[t]); bhi[1] = max(bhi[1], ry[t]);
+        blo[2] = min(blo[2], rz[t]); bhi[2] = max(bhi[2], rz[t]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { blo[k] = warp_min(blo[k]); bhi[k] = warp_max(bhi[k]); }
+
+    // evaluate the n entries ending at queue position `end`
+    auto eval_bodies = [&](int end, int nb) {
+      if (lane < nb) {
+        const int p = S.bodyq[end - nb + lane];
+        const double4 s = a.spos[p];
+        T *w = S.stage + lane * 4;
+        w[0] = (T)((s.x - gc[0]) * inv_s);
+        w[1] = (T)((s.y - gc[1]) * inv_s);
+        w[2] = (T)((s.z - gc[2]) * inv_s);
+        w[3] = (T)(s.w * inv_m);
+      }
+      __syncwarp();
+      T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+      for (int j = 0; j < nb; ++j) {
+        const T *w = S.stage + j * 4;
+        const T sx = w[0], sy = w[1], sz = w[2], sm = w[3];
+#pragma unroll
+        for (int t = 0; t < TPL; ++t) {
+          const T dx = sx - rx[t], dy = sy - ry[t], dz = sz - rz[t];
+          const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+          const T ri = Ops<T>::rsq(r2);
+          const T f = sm * ri * ri * ri;
+          bx[t] = fma(f, dx, bx[t]); by[t] = fma(f, dy, by[t]); bz[t] = fma(f, dz, bz[t]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        if (kKahan) {
+          kahan_add(ax[t], cx[t], bx[t]); kahan_add(ay[t], cy[t], by[t]); kahan_add(az[t], cz[t], bz[t]);
+        } else {
+          ax[t] += bx[t]; ay[t] += by[t]; az[t] += bz[t];
+        }
+      }
+      n_pp += (unsigned long long)nb * gn;
+      __syncwarp();
+    };
+    auto eval_cells = [&](int end, int nc) {
+      if (lane < nc) stage_cell<T, ORDER>(S.stage + lane * W, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
+      __syncwarp();
+      T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+      for (int j = 0; j < nc; ++j) {
+        T w[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) w[k] = S.stage[j * W + k];
+#pragma unroll
+        for (int t = 0; t < TPL; ++t) cell_force<T, ORDER>(w, rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        if (kKahan) {
+          kahan_add(ax[t], cx[t], bx[t]); kahan_add(ay[t], cy[t], by[t]); kahan_add(az[t], cz[t], bz[t]);
+        } else {
+          ax[t] += bx[t]; ay[t] += by[t]; az[t] += bz[t];
+        }
+      }
+      n_pc += (unsigned long long)nc * gn;
+      __syncwarp();
+    };
+
+    int top = 1, ncell = 0, nbody = 0;
+    // a tree visits every node at most once per group: more tests than nodes
+    // means a malformed tree, and the walk stops with an error instead of
+    // looping
+    const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
+    int64_t group_tests = 0;
+    if (lane == 0) stack[0] = 0;
+    __syncwarp();
+    while (top > 0) {
+      if (group_tests > max_tests) { err |= kErrIndex; break; }
+      const int take = min(top, kWarp);
+      const int base = top - take;
+      const int node = lane < take ? stack[base + lane] : -1;
+      top = base;
+      __syncwarp();
+      int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
+      int4 mt = make_int4(0, 0, 0, 0);
+      if (node >= 0) {
+        mt = a.meta[node];
+        const double4 c = a.com[node];
+        const T dx = (T)((c.x - gc[0]) * inv_s), dy = (T)((c.y - gc[1]) * inv_s),
+                dz = (T)((c.z - gc[2]) * inv_s);
+        const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
+        const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
+        const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
+        const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
+        const T size2 = (T)ldexp(1.0, -2 * mt.z);
+        if (size2 <= theta2 * d2) cls = 1;
+        else if (mt.y <= a.leaf_cap || mt.w == 0) cls = 2;
+        else cls = 3;
+      }
+      n_tests += take;
+      group_tests += take;
+      // cells
+      const unsigned cm = __ballot_sync(kFull, cls == 1);
+      if (cls == 1) S.cellq[ncell + __popc(cm & lt)] = node;
+      ncell += __popc(cm);
+      // children of opened internal nodes
+      int32_t ch[8];
+      int nnc = 0, npc = 0;
+      if (cls == 3) {
+        const int4 *cp = reinterpret_cast<const int4 *>(a.child + 8 * (int64_t)node);
+        const int4 c0 = cp[0], c1 = cp[1];
+        ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
+        ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < mt.w) { if (ch[c] >= 0) ++nnc; else ++npc; }
+      }
+      int tot;
+      const int soff = warp_excl_scan(nnc, lane, tot);
+      if (top + tot > stack_cap) {
+        // capacity exceeded: the group's result is incomplete and flagged;
+        // the host repeats the walk with a larger stack
+        err |= kErrStackOverflow;
+      } else {
+        if (cls == 3) {
+          int k = top + soff;
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < mt.w && ch[c] >= 0) stack[k++] = ch[c];
+        }
+        top += tot;
+      }
+      // bodies: lone-particle children (<= 8, one pass) and leaf ranges
+      int rf = 0, rn = 0;
+      if (cls == 2) { rf = mt.x; rn = mt.y; }
+      bool first_pass = true;
+      for (;;) {
+        int give;
+        if (first_pass && cls == 3) give = npc;
+        else give = min(rn, kBodyPerLane);
+        int btot;
+        const int boff = warp_excl_scan(give, lane, btot);
+        if (btot == 0) break;
+        if (first_pass && cls == 3) {
+          int k = nbody + boff;
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < mt.w && ch[c] < 0) S.bodyq[k++] = ~ch[c];
+        } else {
+          for (int k = 0; k < give; ++k) S.bodyq[nbody + boff + k] = rf + k;
+          rf += give; rn -= give;
+        }
+        first_pass = false;
+        nbody += btot;
+        __syncwarp();
+        while (nbody >= kWarp) { eval_bodies(nbody, kWarp); nbody -= kWarp; }
+      }
+      __syncwarp();
+      while (ncell >= kWarp) { eval_cells(ncell, kWarp); ncell -= kWarp; }
+      __syncwarp();
+    }
+    if (ncell > 0) eval_cells(ncell, ncell);
+    if (nbody > 0) eval_bodies(nbody, nbody);
+
+    // write forces in the original order
+    const double scale = a.G * Mtot * inv_s * inv_s;
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) {
+      if (!valid[t]) continue;
+      const int i = gf + lane + kWarp * t;
+      const int p = a.perm[i];
+      double fxs = (double)ax[t], fys = (double)ay[t], fzs = (double)az[t];
+      if (kKahan) { fxs -= (double)cx[t]; fys -= (double)cy[t]; fzs -= (double)cz[t]; }
+      double sc = scale;
+      if (a.out_kind == 0) sc *= a.spos[i].w;
+      a.out[p] = fxs * sc;
+      a.out[a.n + p] = fys * sc;
+      a.out[2 * a.n + p] = fzs * sc;
+    }
+  }
+  if (err && lane == 0) atomicOr(&a.sc->err, err);
+  if (a.count_stats) {
+    // per target: every body/cell batch entry interacts with each valid target
+    // of the group; counted per warp as entries x 1 and scaled on the host
+    if (lane == 0) {
+      atomicAdd(&a.stats[0], n_pp);
+      atomicAdd(&a.stats[1], n_pc);
+      atomicAdd(&a.stats[3], n_tests);
+    }
+  }
+}
+
+// ---- reference-semantics walk (FP64, one thread per target) ----
+
+__device__ __forceinline__ void ref_pp(double bx, double by, double bz, double bm, double qp0,
+                                       double qp1, double qp2, double mp, double G, double eps2,
+                                       double &fx, double &fy, double &fz) {
+  // morton_octree.f90:676-686
+  const double dx = bx - qp0, dy = by - qp1, dz = bz - qp2;
+  const double dist2 = dx * dx + dy * dy + dz * dz + eps2;
+  double inv = 1.0 / sqrt(dist2);
+  inv = inv * inv * inv;
+  const double f = G * mp * bm * inv;
+  fx = fx + f * dx; fy = fy + f * dy; fz = fz + f * dz;
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t nt,
+                      const int32_t *__restrict__ inv_perm, int64_t *__restrict__ counts) {
+  const int L = a.sc->L;
+  const double ssa = a.sc->ssa;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    if (targets && (targets[k] < 0 || targets[k] >= a.n)) {
+      a.out[k] = a.out[nt + k] = a.out[2 * nt + k] = nan("");
+      if (counts) counts[2 * k] = counts[2 * k + 1] = -1;
+      continue;
+    }
+    const int p = targets ? inv_perm[targets[k]] : (int)k;
+    const double4 q = a.spos[p];
+    const double qp0 = q.x, qp1 = q.y, qp2 = q.z, mp = q.w;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    int64_t npp = 0, npc = 0;
+    // stack entries: node j >= 0; lone particle b as ~b (monopole at m q / m);
+    // level-L lone particle b as ~b - 2^30 (summed at its exact position)
+    int32_t st[8 * (kMaxDepth + 2) + 8];
+    int top = 0;
+    st[top++] = 0;
+    const int64_t max_pops = (int64_t)a.sc->n_compact + a.n + 8;
+    int64_t pops = 0;
+    while (top > 0) {
+      if (++pops > max_pops) { atomicOr(&a.sc->err, kErrIndex); break; }
+      const int32_t e = st[--top];
+      if (e < 0) {
+        const bool exact = e < -(1 << 30);
+        const int b = exact ? ~(e + (1 << 30)) : ~e;
+        if (b == p) continue;
+        const double4 s = a.spos[b];
+        if (exact) {
+          ref_pp(s.x, s.y, s.z, s.w, qp0, qp1, qp2, mp, a.G, a.eps2, fx, fy, fz);
+        } else {
+          // single-particle node: qcm = (m q) / m (morton_octree.f90:446-458)
+          const double cx = (s.w * s.x) / s.w, cy = (s.w * s.y) / s.w, cz = (s.w * s.z) / s.w;
+          if (s.w > 0) ref_pp(cx, cy, cz, s.w, qp0, qp1, qp2, mp, a.G, a.eps2, fx, fy, fz);
+        }
+        ++npp;
+        continue;
+      }
+      const int4 mt = a.meta[e];
+      if (mt.w == 0) {  // level-L leaf: particle by particle (:672-691)
+        for (int b = mt.x; b < mt.x + mt.y; ++b) {
+          if (b == p) continue;
+          const double4 s = a.spos[b];
+          ref_pp(s.x, s.y, s.z, s.w, qp0, qp1, qp2, mp, a.G, a.eps2, fx, fy, fz);
+          ++npp;
+        }
+        continue;
+      }
+      bool open = (mt.x <= p && p < mt.x + mt.y);  // :694-697
+      if (!open) {
+        const double4 c = a.com[e];
+        const double dx = c.x - qp0, dy = c.y - qp1, dz = c.z - qp2;
+        double dist2 = dx * dx + dy * dy + dz * dz;
+        const double size = ssa * ldexp(1.0, -mt.z);
+        if (size * size <= a.theta2 * dist2) {  // :706
+          if (c.w > 0) {
+            dist2 = dist2 + a.eps2;
+            if (ORDER < 4) {
+              double inv = 1.0 / sqrt(dist2);
+              inv = inv * inv * inv;
+              const double f = a.G * mp * c.w * inv;
+              fx = fx + f * dx; fy = fy + f * dy; fz = fz + f * dz;
+            } else {  // :721-753
+              const double *Q = a.quad + 6 * (int64_t)e;
+              const double invR = 1.0 / sqrt(dist2);
+              const double invR2 = 1.0 / dist2;
+              const double invR3 = invR * invR2;
+              const double invR5 = invR3 * invR * invR;
+              const double mx = dx * invR3 * c.w, my = dy * invR3 * c.w, mz = dz * invR3 * c.w;
+              const double dx2 = 15.0 * dx * dx * invR2 - 3.0;
+              const double dy2 = 15.0 * dy * dy * invR2 - 3.0;
+              const double dz2 = 15.0 * dz * dz * invR2 - 3.0;
+              const double dxyz = 15.0 * dx * dy * dz * invR2;
+              double Qx = (Q[0] * (dx2 - 6.0) + Q[1] * dy2 + Q[2] * dz2) * 0.5 * dx;
+              double Qy = (Q[1] * (dy2 - 6.0) + Q[2] * dz2 + Q[0] * dx2) * 0.5 * dy;
+              double Qz = (Q[2] * (dz2 - 6.0) + Q[0] * dx2 + Q[1] * dy2) * 0.5 * dz;
+              Qx = Qx + Q[3] * dy * dx2 + Q[4] * dz * dx2 + Q[5] * dxyz;
+              Qy = Qy + Q[5] * dz * dy2 + Q[3] * dx * dy2 + Q[4] * dxyz;
+              Qz = Qz + Q[4] * dx * dz2 + Q[5] * dy * dz2 + Q[3] * dxyz;
+              if (ORDER < 8) {
+                fx = fx + a.G * mp * (mx + invR5 * Qx);
+                fy = fy + a.G * mp * (my + invR5 * Qy);
+                fz = fz + a.G * mp * (mz + invR5 * Qz);
+              } else {  // octupole terms of octree_default.f90:1012-1063
+                const double *o = a.oct + 14 * (int64_t)e;
+                const double invR7 = invR5 * invR * invR;
+                const double invR9 = invR7 * invR * invR;
+                double Ox = -1.5 * invR5 * o[11], Oy = -1.5 * invR5 * o[12], Oz = -1.5 * invR5 * o[13];
+                double Oc = 7.5 * invR7 * (dx * o[11] + dy * o[12] + dz * o[13]);
+                Ox = Ox + dx * Oc; Oy = Oy + dy * Oc; Oz = Oz + dz * Oc;
+                const double ddx = dx * dx, ddy = dy * dy, ddz = dz * dz;
+                Ox = Ox + 7.5 * invR7 * (ddx * o[0] + ddy * o[1] + ddz * o[2] + 2.0 * dx * dy * o[3] +
+                                         2.0 * dx * dz * o[6] + 2.0 * dy * dz * o[9]);
+                Oy = Oy + 7.5 * invR7 * (ddx * o[3] + ddy * o[4] + ddz * o[5] + 2.0 * dx * dy * o[1] +
+                                         2.0 * dx * dz * o[9] + 2.0 * dy * dz * o[7]);
+                Oz = Oz + 7.5 * invR7 * (ddx * o[6] + ddy * o[7] + ddz * o[8] + 2.0 * dx * dy * o[9] +
+                                         2.0 * dx * dz * o[2] + 2.0 * dy * dz * o[5]);
+                Oc = -17.5 * invR9 *
+                     (ddx * dx * o[0] + ddy * dy * o[4] + ddz * dz * o[8] + 3.0 * ddx * dy * o[3] +
+                      3.0 * ddx * dz * o[6] + 3.0 * ddy * dx * o[1] + 3.0 * ddy * dz * o[7] +
+                      3.0 * ddz * dx * o[2] + 3.0 * ddz * dy * o[5] + 6.0 * dx * dy * dz * o[9]);
+                Ox = Ox + dx * Oc; Oy = Oy + dy * Oc; Oz = Oz + dz * Oc;
+                fx = fx + a.G * mp * (mx + invR5 * Qx + Ox);
+                fy = fy + a.G * mp * (my + invR5 * Qy + Oy);
+                fz = fz + a.G * mp * (mz + invR5 * Qz + Oz);
+              }
+            }
+          }
+          ++npc;
+          continue;
+        }
+      }
+      // open: push children in reverse so they pop in key order
+      const bool deepest = (mt.z + 1 == L);
+      for (int c = mt.w - 1; c >= 0; --c) {
+        const int32_t ch = a.child[8 * (int64_t)e + c];
+        if (top >= (int)(sizeof(st) / sizeof(st[0]))) break;
+        st[top++] = (ch < 0 && deepest) ? ch - (1 << 30) : ch;
+      }
+    }
+    const int orig = a.perm[p];
+    double sc = 1.0;
+    if (a.out_kind == 1) sc = 1.0 / mp;
+    if (targets) {
+      a.out[k] = fx * sc; a.out[nt + k] = fy * sc; a.out[2 * nt + k] = fz * sc;
+    } else {
+      a.out[orig] = fx * sc; a.out[a.n + orig] = fy * sc; a.out[2 * a.n + orig] = fz * sc;
+    }
+    if (counts) { counts[2 * k] = npp; counts[2 * k + 1] = npc; }
+  }
+}
+
+int g_sm_count = 0;
+
+}  // namespace
+
+int64_t walk_slots() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return (int64_t)g_sm_count * 8 * kWalkWarps;
+}
+
+template <typename T, int ORDER, int TPL>
+static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
+  const int blocks = (int)(walk_slots() / kWalkWarps);
+  group_walk_kernel<T, ORDER, TPL><<<blocks, kWalkWarps * kWarp, 0, s>>>(a);
+}
+
+static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *out) {
+  WalkArgs a;
+  a.meta = b.cn_meta; a.child = b.cn_child; a.com = b.cn_com; a.quad = b.cn_quad; a.oct = b.cn_oct;
+  a.fq = b.cn_fq; a.fo = b.cn_fo; a.spos = b.spos; a.perm = b.v0; a.g_first = b.g_first;
+  a.sc = b.sc; a.cursor = b.counters; a.stack = b.wstack; a.stack_cap = b.wstack_cap;
+  a.stats = b.stats; a.out = out; a.n = n;
+  a.theta2 = p.theta2; a.G = p.G; a.eps2 = p.eps2;
+  a.out_kind = p.out_kind; a.leaf_cap = p.leaf_cap; a.count_stats = p.count_stats;
+  return a;
+}
+
+void launch_walk(int64_t n, const WalkParams &p, Buffers &b, double *out, cudaStream_t s) {
+  WalkArgs a = make_args(n, p, b, out);
+  cudaMemsetAsync(b.counters, 0, sizeof(int32_t), s);
+  const bool two = p.group_size > 32;
+#define BH_WALK(T, O)                                                   \
+  do {                                                                  \
+    if (two) launch_group_walk<T, O, 2>(a, s);                          \
+    else launch_group_walk<T, O, 1>(a, s);                              \
+  } while (0)
+  if (p.precision == BH_PREC_FP64) {
+    if (p.order >= 8) BH_WALK(double, 8);
+    else if (p.order >= 4) BH_WALK(double, 4);
+    else BH_WALK(double, 1);
+  } else {
+    if (p.order >= 8) BH_WALK(float, 8);
+    else if (p.order >= 4) BH_WALK(float, 4);
+    else BH_WALK(float, 1);
+  }
+#undef BH_WALK
+}
+
+__global__ void inv_perm_kernel(const int32_t *__restrict__ perm, int64_t n, int32_t *__restrict__ inv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    inv[perm[i]] = (int32_t)i;
+}
+
+void launch_reference_walk(int64_t n, const WalkParams &p, Buffers &b, double *out,
+                           const int64_t *targets, int64_t ntargets, int64_t *counts,
+                           cudaStream_t s) {
+  WalkArgs a = make_args(n, p, b, out);
+  int32_t *inv = nullptr;
+  if (targets) {
+    inv = b.gscan;  // free after the group pass
+    inv_perm_kernel<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(b.v0, n, inv);
+  }
+  const int64_t nt = targets ? ntargets : n;
+  const int grid = grid_for(nt, 128, 148 * 32);
+  if (p.order >= 8)
+    reference_walk_kernel<8><<<grid, 128, 0, s>>>(a, targets, nt, inv, counts);
+  else if (p.order >= 4)
+    reference_walk_kernel<4><<<grid, 128, 0, s>>>(a, targets, nt, inv, counts);
+  else
+    reference_walk_kernel<1><<<grid, 128, 0, s>>>(a, targets, nt, inv, counts);
+}
+
+}  // namespace bh

@@ -1,0 +1,157 @@
+/*
+ * hierarquicos_bh.h -- C ABI of the B200 Barnes-Hut force engine.
+ *
+ * Plain C types only: host or device pointers to float64 arrays, sizes as
+ * int64_t, and an optional CUDA stream passed as void* (NULL = the legacy
+ * default stream).  Every function returns a status code (BH_OK on success);
+ * bh_last_error() gives the message of the last failure on the calling thread.
+ *
+ * Layout conventions, matching the reference's f2py module api_mod:
+ *  - inputs are four separate float64 vectors m, x, y, z of length n;
+ *  - results are written SoA, out[0..n) = fx, out[n..2n) = fy,
+ *    out[2n..3n) = fz, which is the memory layout of the Fortran (N,3) array
+ *    that api_mod.compute_forces returns;
+ *  - theta and eps are passed unsquared and squared inside, as
+ *    parareal/api3d.f90:30 does.
+ */
+#ifndef HIERARQUICOS_BH_H
+#define HIERARQUICOS_BH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define BH_OK 0
+#define BH_ERR_INVALID 1     /* bad argument (size, order, depth, pointer)          */
+#define BH_ERR_CUDA 2        /* CUDA runtime error                                 */
+#define BH_ERR_NOMEM 3       /* device allocation failed                           */
+#define BH_ERR_NONFINITE 4   /* NaN/Inf input or zero total mass                   */
+#define BH_ERR_CAPACITY 5    /* walk stack capacity exceeded (after retries)        */
+#define BH_ERR_DUPLICATES 6  /* depth 0 asked but coincident bodies never separate  */
+#define BH_ERR_INTERNAL 7    /* an internal consistency check failed               */
+#define BH_ERR_NOT_BUILT 8   /* system queried before a successful build           */
+
+/* ---- walk precision ---- */
+#define BH_PREC_FP32 0       /* warp-cooperative group walk, FP32, Kahan-compensated */
+#define BH_PREC_FP64 1       /* the same group walk in FP64                          */
+#define BH_PREC_REFERENCE 2  /* per-target FP64 walk with the reference's MAC        */
+
+typedef struct bh_params {
+    double theta;     /* opening angle, unsquared                                 */
+    double G;         /* gravitational constant                                   */
+    double eps;       /* softening length, unsquared                              */
+    int order;        /* 1 monopole, 4 quadrupole, 8 octupole                     */
+    int out_kind;     /* 0 forces G m_i a_i, 1 accelerations G a_i                */
+    int depth;        /* Morton depth L in 1..21; 0 = smallest depth with unique keys */
+    int precision;    /* BH_PREC_*                                                */
+    double amp;       /* root cube side = amp * largest extent (reference: 1.2)   */
+    int group_size;   /* targets per warp in the group walk: 32 or 64             */
+    int leaf_cap;     /* nodes with <= leaf_cap bodies are opened into bodies (1..16) */
+    int com_mode;     /* centre of mass for the keys: 0 separately rounded m*q,
+                         1 fused multiply-add (what gfortran -O3 -march=native emits) */
+    int strict_keys;  /* 1: recompute the centre of mass in the reference's sequential
+                         order and re-run the build if any key differs            */
+    int reserved[4];
+} bh_params;
+
+/* Defaults: theta 0.5, G 1, eps 0, order 4, forces, depth 21, FP32, amp 1.2,
+ * group 64, leaf_cap 8, com_mode 1, strict_keys 1. */
+void bh_params_default(bh_params *p);
+
+const char *bh_version(void);
+int bh_last_error(char *buf, int len);
+
+/* Drop-in for api_mod.compute_forces (fortran/api3d.f90:20-41; REAL(16) twin
+ * parareal/api3d.f90:20-44): host arrays in, forces (N,3) out, every call a
+ * fresh tree.  order: 1 monopole, 4 quadrupole (the f2py quad=.TRUE.), 8
+ * octupole.  out_kind 0 forces, 1 accelerations. */
+int bh_compute_forces(const double *m, const double *x, const double *y, const double *z,
+                      int64_t n, double theta, double G, double eps, int order, int out_kind,
+                      double *out, void *stream);
+
+/* bh_compute_forces with every parameter (host arrays). */
+int bh_compute_forces_ex(const double *m, const double *x, const double *y, const double *z,
+                         int64_t n, const bh_params *p, double *out, void *stream);
+
+/* Drop-in for api_mod.compute_forces_direct (fortran/api3d.f90:43-72) and
+ * direct_forces_mod.compute_forces_direct (fortran/direct_forces.f90:8-63):
+ * FP64 O(N^2) sum on the device.  Host arrays. */
+int bh_compute_forces_direct(const double *m, const double *x, const double *y,
+                             const double *z, int64_t n, double G, double eps, int out_kind,
+                             double *out, void *stream);
+
+/* FP64 direct sum on a subset of targets, DEVICE arrays: out is SoA over the
+ * ntargets targets (original indices in d_targets).  Used for error checks. */
+int bh_direct_targets_device(const double *d_m, const double *d_x, const double *d_y,
+                             const double *d_z, int64_t n, const int64_t *d_targets,
+                             int64_t ntargets, double G, double eps, int out_kind, double *d_out,
+                             void *stream);
+
+/* ---- device-resident systems (replaces OctreeType / morton_tree_type:
+ *      pre_init + init, octree_default.f90:178-387, morton_octree.f90:73-111) ---- */
+typedef struct bh_system bh_system;
+
+int bh_system_create(bh_system **sys, int device);
+int bh_system_destroy(bh_system *sys);
+
+/* Keys, sort, octree and multipoles for DEVICE arrays (morton_octree.f90:328-625,
+ * octree_default.f90:744-882).  Asynchronous on `stream`. */
+int bh_system_build(bh_system *sys, const double *d_m, const double *d_x, const double *d_y,
+                    const double *d_z, int64_t n, const bh_params *p, void *stream);
+
+/* Tree walk over the built tree (octree_default.f90:1811-2095 grouped walk;
+ * morton_octree.f90:627-766 with BH_PREC_REFERENCE); d_out SoA n x 3 in the
+ * ORIGINAL particle order.  Asynchronous. */
+int bh_system_walk(bh_system *sys, const bh_params *p, double *d_out, void *stream);
+
+/* build + walk + bh_system_sync: the device-array form of bh_compute_forces. */
+int bh_system_forces(bh_system *sys, const double *d_m, const double *d_x, const double *d_y,
+                     const double *d_z, int64_t n, const bh_params *p, double *d_out,
+                     void *stream);
+
+/* Waits for the stream and turns device-side error flags into a status. */
+int bh_system_sync(bh_system *sys, void *stream);
+
+/* After a build: particle count, depth L, compact node count, group count,
+ * centre of mass + total mass (com4), root cube side. Synchronises. */
+int bh_system_info(bh_system *sys, int64_t *n, int *depth, int64_t *n_nodes, int64_t *n_groups,
+                   double *com4, double *ssa);
+
+/* Sorted Morton keys and the permutation (sorted position -> original index),
+ * copied to HOST buffers of n entries (morton_octree.f90:404-417). */
+int bh_system_get_keys(bh_system *sys, uint64_t *keys, int32_t *perm);
+
+/* Compact octree copied to HOST buffers (any pointer may be NULL), node count
+ * from bh_system_info.  meta4: first, count, level, nchild per node; child8:
+ * 8 per node, >= 0 a node, < 0 the particle ~c at sorted position; com4:
+ * x, y, z, mass; quad6: xx yy zz xy xz yz; oct14: octree_default.f90 layout;
+ * level_begin: L + 2 entries. */
+int bh_system_get_nodes(bh_system *sys, int32_t *meta4, int32_t *child8, int32_t *parent,
+                        double *com4, double *quad6, double *oct14, int32_t *level_begin);
+
+/* Group ranges (first sorted particle of each group), n_groups + 1 entries. */
+int bh_system_get_groups(bh_system *sys, int32_t *group_first);
+
+/* Interaction counters of the last walk with counting enabled (reserved[0] = 1
+ * in bh_params): [0] body-body, [1] body-cell, [2] groups, [3] node tests. */
+int bh_system_get_stats(bh_system *sys, uint64_t *stats4);
+
+/* Per-target FP64 walk with the reference's semantics on a subset of targets
+ * (DEVICE arrays, original indices); counts (optional, device, 2 per target):
+ * body-body and cell interactions. */
+int bh_system_reference_targets(bh_system *sys, const bh_params *p, const int64_t *d_targets,
+                                int64_t ntargets, double *d_out, int64_t *d_counts,
+                                void *stream);
+
+/* FP32 and FP64 fused-multiply-add throughput probe (independent chains,
+ * CUDA events): writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64). */
+int bh_probe_fma_peak(int device, double *gflops2);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HIERARQUICOS_BH_H */

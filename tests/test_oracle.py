@@ -1,0 +1,116 @@
+"""The CPU oracle: pinned against the reference's recorded error statistics,
+internally consistent, and reproducing its committed golden vectors."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import plummer, xyz
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def recorded():
+    with open(os.path.join(GOLDEN, "recorded_errors.json")) as f:
+        return json.load(f)
+
+
+def _normalised_rms(oracle_mod, m, q, f, fd):
+    from oracle.metrics import normalised_rms
+
+    return normalised_rms(m, q, f, fd)
+
+
+@pytest.mark.parametrize("order,method", [(1, 10), (4, 11), (8, 12)])
+def test_oracle_matches_recorded_error_statistics(oracle_mod, recorded, order, method):
+    """Statistical pin: the reference's aarseth runs (Plummer, size 10,
+    b = 0.58, eps = 0, N = 1024) recorded the normalised RMS error of methods
+    10/11/12; the oracle's median over 7 seeded draws must fall inside
+    [0.6 x p10, 1.6 x p90] of the recorded draws at every theta."""
+    from hierarquicos_b200.initial_values import generate_initial_values
+
+    n = 1024
+    thetas = [0.2, 0.3, 0.5, 0.7, 1.0]
+    errs = {th: [] for th in thetas}
+    for seed in range(7):
+        m, q, _ = generate_initial_values(n, 10.0, 0.0, True, False, "plummer", (1.0, 0.58),
+                                          seed=100 + seed, velocities=False)
+        x, y, z = xyz(q)
+        fd = oracle_mod.direct_forces(m, x, y, z, 1.0, 0.0)
+        tree = oracle_mod.Octree(m, method).init(x, y, z)
+        for th in thetas:
+            f = tree.forces(th * th, 1.0, 0.0)
+            errs[th].append(_normalised_rms(oracle_mod, m, q, f, fd))
+    for th in thetas:
+        rec = recorded[f"{order}/{n}/{th:.1f}"]
+        med = float(np.median(errs[th]))
+        assert 0.6 * rec["p10"] <= med <= 1.6 * rec["p90"], (order, th, med, rec)
+
+
+def test_morton_and_insertion_walks_agree(oracle_mod):
+    """The Morton walk (morton_octree.f90:627-766) and the insertion-tree walk
+    (octree_default.f90:895-1078) see the same cube and the same MAC."""
+    m, q = plummer(2048, seed=5)
+    x, y, z = xyz(q)
+    for quad, method in ((False, 10), (True, 11)):
+        fm = oracle_mod.MortonTree(m, x, y, z, 21, 1.2, quad).forces_par(1.0, 1e-4, 0.25, quad)
+        fo = oracle_mod.Octree(m, method).init(x, y, z).forces(0.25, 1.0, 1e-4)
+        rel = np.linalg.norm(fm - fo, axis=1) / np.linalg.norm(fo, axis=1)
+        assert np.median(rel) < 1e-12 and rel.max() < 1e-6
+
+
+def test_grouped_walk_is_at_least_as_accurate(oracle_mod):
+    m, q = plummer(4096, seed=6)
+    x, y, z = xyz(q)
+    fd = oracle_mod.direct_forces(m, x, y, z, 1.0, 1e-4)
+    for a, b in ((10, 30), (11, 31), (12, 32)):
+        fa = oracle_mod.Octree(m, a).init(x, y, z).forces(0.25, 1.0, 1e-4)
+        fb = oracle_mod.Octree(m, b).init(x, y, z).forces(0.25, 1.0, 1e-4)
+        ea = np.linalg.norm(fa - fd) / np.linalg.norm(fd)
+        eb = np.linalg.norm(fb - fd) / np.linalg.norm(fd)
+        assert eb <= ea * 1.05
+
+
+def test_direct_sum_conserves_momentum(oracle_mod):
+    m, q = plummer(500, seed=2)
+    fd = oracle_mod.direct_forces(m, *xyz(q), 1.0, 1e-4)
+    assert np.abs(fd.sum(axis=0)).max() < 1e-14 * np.abs(fd).sum()
+    ft = oracle_mod.direct_forces_targets(m, *xyz(q), np.arange(500), 1.0, 1e-4)
+    np.testing.assert_allclose(ft, fd, rtol=1e-12, atol=1e-15 * np.abs(fd).max())
+
+
+def test_argsort_is_stable(oracle_mod):
+    rng = np.random.default_rng(0)
+    keys = rng.integers(0, 50, 10000).astype(np.uint64)
+    perm = oracle_mod.argsort(keys)
+    assert np.array_equal(perm, np.argsort(keys, kind="stable"))
+
+
+def test_oracle_reproduces_golden_vectors(oracle_mod):
+    g = np.load(os.path.join(GOLDEN, "oracle_small.npz"))
+    t10 = oracle_mod.MortonTree(g["m10"], g["x10"], g["y10"], g["z10"], L=0, ssa=1.2,
+                                use_quadrupole=True, fma_mode=1)
+    assert t10.L == int(g["L10"])
+    k, p = t10.sorted()
+    assert np.array_equal(k, g["keys10"]) and np.array_equal(p, g["perm10"])
+    assert np.array_equal(t10.forces_par(1.0, 1e-4, 0.01, True), g["forces10"])
+    t = oracle_mod.MortonTree(g["m"], g["x"], g["y"], g["z"], L=21, ssa=1.2, use_quadrupole=True,
+                              fma_mode=1)
+    k, p = t.sorted()
+    assert np.array_equal(k, g["keys"]) and np.array_equal(p, g["perm"])
+    assert np.array_equal(t.forces_par(1.0, 1e-4, 0.25, True), g["forces_morton_quad"])
+    fo = oracle_mod.Octree(g["m"], 12).init(g["x"], g["y"], g["z"]).forces(0.25, 1.0, 1e-4)
+    assert np.array_equal(fo, g["forces_octupole"])
+    fd = oracle_mod.direct_forces(g["m"], g["x"], g["y"], g["z"], 1.0, 1e-4)
+    assert np.array_equal(fd, g["forces_direct"])
+
+
+def test_keys_fma_modes_differ_only_near_cell_edges(oracle_mod):
+    # the two centre-of-mass roundings give the same keys unless a body sits
+    # within rounding distance of a 2^-21 cell boundary
+    m, q = plummer(20000, seed=9)
+    k0, *_ = oracle_mod.morton_keys(m, *xyz(q), 21, 1.2, 0)
+    k1, *_ = oracle_mod.morton_keys(m, *xyz(q), 21, 1.2, 1)
+    assert np.mean(k0 == k1) > 0.999
