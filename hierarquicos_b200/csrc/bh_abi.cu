@@ -16,13 +16,15 @@ struct bh_system {
   Buffers b;
   int64_t n = 0;
   int built = 0;
-  int verify_pending = 0;
+  int keys_checked = 0;   // strict-key check done for the current build
   int order = 4;
   int64_t stack_cap = 4096;
-  cudaStream_t side = nullptr;
-  cudaEvent_t side_done = nullptr;
   const double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
   bh_params p{};
+  // the last walk of the current build, repeated if the build is redone
+  int walked = 0;
+  bh_params walk_p{};
+  double *walk_out = nullptr;
 };
 
 namespace {
@@ -133,6 +135,7 @@ int check_params(const bh_params *p, int64_t n) {
   if (p->leaf_cap < 1 || p->leaf_cap > 64) return set_err(BH_ERR_INVALID, "leaf_cap must be in 1..64");
   if (p->out_kind != 0 && p->out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
   if (p->com_mode != 0 && p->com_mode != 1) return set_err(BH_ERR_INVALID, "com_mode must be 0 or 1");
+  if (p->strict_keys < 0 || p->strict_keys > 2) return set_err(BH_ERR_INVALID, "strict_keys must be 0, 1 or 2");
   return BH_OK;
 }
 
@@ -166,8 +169,7 @@ void enqueue_build(bh_system *s, int64_t n, int keys_from_scalars, cudaStream_t 
   if (keys_from_scalars)
     bh::launch_keys_only(s->x, s->y, s->z, n, L, b, st);
   else
-    bh::launch_keys(s->m, s->x, s->y, s->z, n, L, p.amp, p.com_mode, p.strict_keys, b, st, s->side,
-                    s->side_done);
+    bh::launch_keys(s->m, s->x, s->y, s->z, n, L, p.amp, p.com_mode, b, st);
   const int bits = (L == 0) ? 3 * bh::kMaxDepth : 3 * L;
   bh::radix_sort_pairs(b.k0, b.v0, b.k1, b.v1, n, nullptr, bits, b.hist, st);
   if (L == 0) bh::launch_auto_depth(n, b, st);
@@ -248,11 +250,6 @@ int bh_system_create(bh_system **sys, int device) {
   bh_system *s = new bh_system();
   s->device = device;
   bh_params_default(&s->p);
-  if (cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->side_done, cudaEventDisableTiming) != cudaSuccess) {
-    delete s;
-    return set_err(BH_ERR_CUDA, "stream/event creation failed");
-  }
   bh::set_seq_com_smem_limit();
   *sys = s;
   return BH_OK;
@@ -263,8 +260,6 @@ int bh_system_destroy(bh_system *s) {
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
   free_buffers(s->b);
-  if (s->side) cudaStreamDestroy(s->side);
-  if (s->side_done) cudaEventDestroy(s->side_done);
   delete s;
   return BH_OK;
 }
@@ -283,17 +278,18 @@ int bh_system_build(bh_system *s, const double *d_m, const double *d_x, const do
   s->m = d_m; s->x = d_x; s->y = d_y; s->z = d_z;
   s->n = n;
   s->order = p->order;
+  s->walked = 0;
   if (n == 1) {
     // a lone body feels no force; there is no extent to normalise by
     BH_CUDA(cudaMemsetAsync(s->b.sc, 0, sizeof(bh::Scalars), st));
     s->built = 1;
-    s->verify_pending = 0;
+    s->keys_checked = 1;
     return BH_OK;
   }
   enqueue_build(s, n, 0, st);
   BH_CUDA(cudaGetLastError());
   s->built = 1;
-  s->verify_pending = p->strict_keys ? 1 : 0;
+  s->keys_checked = p->strict_keys ? 0 : 1;
   return BH_OK;
 }
 
@@ -317,27 +313,60 @@ int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream
     else
       bh::launch_walk(n, w, s->b, d_out, st);
   }
-  if (s->verify_pending) {
-    BH_CUDA(cudaStreamWaitEvent(st, s->side_done, 0));
-    bh::launch_verify_keys(s->m, s->x, s->y, s->z, n, p->depth, s->b, st);
-    s->verify_pending = 0;
-  }
+  s->walked = 1;
+  s->walk_p = *p;
+  s->walk_out = d_out;
   BH_CUDA(cudaGetLastError());
   return BH_OK;
 }
 
+namespace {
+
+// Completes a build + walk: strict-key check (slow path only when a body lies
+// within the rounding margin of a cell edge), stack-capacity retries, status.
+int finish(bh_system *s, cudaStream_t st) {
+  int rc = read_scalars(s, st);
+  if (rc) return rc;
+  if (!s->keys_checked && (s->b.sc_host->key_ambiguous || s->p.strict_keys == 2) &&
+      !(s->b.sc_host->err & bh::kErrNonFinite)) {
+    // the reference's sequential centre of mass decides the ambiguous keys
+    bh::launch_seq_com(s->m, s->x, s->y, s->z, s->n, s->p.com_mode, s->b, st);
+    bh::launch_verify_keys(s->m, s->x, s->y, s->z, s->n, s->p.depth, s->b, st);
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+    if (s->b.sc_host->key_mismatch) {
+      bh::launch_adopt_seq_com(s->b, st);
+      enqueue_build(s, s->n, 1, st);
+      if (s->walked) {
+        rc = bh_system_walk(s, &s->walk_p, s->walk_out, st);
+        if (rc) return rc;
+      }
+      rc = read_scalars(s, st);
+      if (rc) return rc;
+    }
+  }
+  s->keys_checked = 1;
+  for (int attempt = 0; attempt < 4 && s->walked && (s->b.sc_host->err & bh::kErrStackOverflow);
+       ++attempt) {
+    s->stack_cap *= 2;
+    rc = ensure_capacity(s, s->n);
+    if (rc) return rc;
+    BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
+    rc = bh_system_walk(s, &s->walk_p, s->walk_out, st);
+    if (rc) return rc;
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+  }
+  return status_from_device(s, 0);
+}
+
+}  // namespace
+
 int bh_system_sync(bh_system *s, void *stream) {
   if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
   BH_CUDA(cudaSetDevice(s->device));
-  cudaStream_t st = (cudaStream_t)stream;
-  if (s->verify_pending && s->built) {
-    BH_CUDA(cudaStreamWaitEvent(st, s->side_done, 0));
-    bh::launch_verify_keys(s->m, s->x, s->y, s->z, s->n, s->p.depth, s->b, st);
-    s->verify_pending = 0;
-  }
-  int rc = read_scalars(s, st);
-  if (rc) return rc;
-  return status_from_device(s, 0);
+  if (!s->built) return set_err(BH_ERR_NOT_BUILT, "sync before build");
+  return finish(s, (cudaStream_t)stream);
 }
 
 int bh_system_forces(bh_system *s, const double *d_m, const double *d_x, const double *d_y,
@@ -347,30 +376,7 @@ int bh_system_forces(bh_system *s, const double *d_m, const double *d_x, const d
   if (rc) return rc;
   rc = bh_system_walk(s, p, d_out, stream);
   if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  rc = read_scalars(s, st);
-  if (rc) return rc;
-  const bh::Scalars &h = *s->b.sc_host;
-  if (h.key_mismatch) {
-    // a key differs from the reference's: rebuild from the sequential-order
-    // centre of mass (the reference's own) and walk again
-    bh::launch_adopt_seq_com(s->b, st);
-    enqueue_build(s, n, 1, st);
-    bh_system_walk(s, p, d_out, stream);
-    rc = read_scalars(s, st);
-    if (rc) return rc;
-  }
-  for (int attempt = 0; attempt < 4 && (s->b.sc_host->err & bh::kErrStackOverflow); ++attempt) {
-    s->stack_cap *= 2;
-    rc = ensure_capacity(s, n);
-    if (rc) return rc;
-    BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
-    rc = bh_system_walk(s, p, d_out, stream);
-    if (rc) return rc;
-    rc = read_scalars(s, st);
-    if (rc) return rc;
-  }
-  return status_from_device(s, 0);
+  return finish(s, (cudaStream_t)stream);
 }
 
 int bh_system_info(bh_system *s, int64_t *n, int *depth, int64_t *n_nodes, int64_t *n_groups,

@@ -40,7 +40,9 @@ struct Scalars {
   int err;                  // DeviceError bits
   int key_mismatch;         // keys differ from the sequential-COM keys
   int max_lcp;              // deepest shared octal prefix (auto depth)
-  int pad[2];
+  int key_ambiguous;        // some body lies within the rounding margin of a cell edge
+  int pad;
+  double key_margin;        // that margin, in units of the finest cell
 };
 
 // Per-system device buffers.  Sized for `cap` particles.
@@ -92,8 +94,9 @@ struct Buffers {
 
 // keys: bbox + COM + keys.  com_mode: 0 separate multiply and add, 1 fused.
 void launch_keys(const double *m, const double *x, const double *y, const double *z, int64_t n,
-                 int L, double amp, int com_mode, int strict, Buffers &b, cudaStream_t s,
-                 cudaStream_t side, cudaEvent_t side_done);
+                 int L, double amp, int com_mode, Buffers &b, cudaStream_t s);
+void launch_seq_com(const double *m, const double *x, const double *y, const double *z,
+                    int64_t n, int com_mode, Buffers &b, cudaStream_t s);
 void launch_verify_keys(const double *m, const double *x, const double *y, const double *z,
                         int64_t n, int L, Buffers &b, cudaStream_t s);
 void launch_auto_depth(int64_t n, Buffers &b, cudaStream_t s);

@@ -2,17 +2,22 @@
 //
 // Follows fortran/morton/morton_octree.f90:359-395 (generate_nodes steps 1-5)
 // and :184-213 (morton_key).  All arithmetic that feeds a key uses explicitly
-// rounded intrinsics so that no multiply-add is contracted and every key is
-// bit-identical to the reference's for the same centre of mass.
+// rounded intrinsics so that no multiply-add is contracted.
 //
-// The reference sums the centre of mass sequentially (:364-370).  A parallel
-// sum may differ in the last bits, and keys depend on those bits only for a
-// body that sits within an ulp of a 2^-21 cell boundary.  The pipeline
-// therefore computes keys from a deterministic parallel sum, and, when strict
-// keys are requested, a side stream recomputes the sum in the reference's
-// order on one thread block; launch_verify_keys then recomputes every key with
-// that centre of mass and flags any difference, in which case the host
-// rebuilds with the sequential centre of mass (see bh_abi.cu).
+// Keys and the centre of mass.  The reference sums the centre of mass c
+// sequentially (:364-370) and normalises x_n = fl(fl(fl(q - c)/ssa) + 0.5) -
+// vcen, vcen = 0.5 fl(vmin + vmax) with vmin/vmax the normalised extremes
+// (:373-384).  In exact arithmetic c cancels: x_n = (q - (qmin+qmax)/2)/ssa +
+// 1/2.  So two evaluations with different roundings of c differ only by their
+// rounding errors, |x_n(c1) - x_n(c2)| <= 2 u (6.02 V + 1.5) with u = 2^-53 and
+// V = max |v| <= 0.84 for non-negative masses (each of the five rounded
+// operations contributes at most u times its operand).  A body whose
+// 2^21 x_n lies farther than that (times a safety factor 1.5) from an integer
+// on every axis therefore gets the reference's key whatever c is.  The keys
+// kernel computes c with a deterministic parallel sum, checks that margin for
+// every body and raises `key_ambiguous` if any body is inside it; only then
+// does the host run the reference's sequential sum (seq_com_kernel) and
+// compare the keys (verify_keys_kernel), rebuilding if one differs.
 #include <math.h>
 
 #include "bh_internal.cuh"
@@ -47,8 +52,16 @@ __device__ __forceinline__ int64_t quantise(double xn, int L) {
   return i;
 }
 
+// fraction of the finest cell: ambiguous when within `margin` of an edge
+__device__ __forceinline__ bool near_edge(double xn, double margin) {
+  const double f = __dmul_rn(xn, 2097152.0);  // exact
+  const double r = f - floor(f);               // exact
+  return r < margin || r > 1.0 - margin;
+}
+
 __device__ __forceinline__ uint64_t key_of(double x, double y, double z, const double com[3],
-                                           double ssa, const double vcen[3], int L, int *bad) {
+                                           double ssa, const double vcen[3], int L, int *bad,
+                                           double margin = -1.0, int *amb = nullptr) {
   // positions_norm = (q - qcm) / ssa, then + 0.5 - ssi (morton_octree.f90:373-384)
   double vx = __ddiv_rn(__dsub_rn(x, com[0]), ssa);
   double vy = __ddiv_rn(__dsub_rn(y, com[1]), ssa);
@@ -57,6 +70,7 @@ __device__ __forceinline__ uint64_t key_of(double x, double y, double z, const d
   double yn = __dsub_rn(__dadd_rn(vy, 0.5), vcen[1]);
   double zn = __dsub_rn(__dadd_rn(vz, 0.5), vcen[2]);
   if (!(xn >= 0.0 && xn < 1.0 && yn >= 0.0 && yn < 1.0 && zn >= 0.0 && zn < 1.0)) *bad = 1;
+  if (amb && (near_edge(xn, margin) || near_edge(yn, margin) || near_edge(zn, margin))) *amb = 1;
   uint64_t ix = (uint64_t)quantise(xn, L), iy = (uint64_t)quantise(yn, L),
            iz = (uint64_t)quantise(zn, L);
   return (spread3(ix) << 2) | (spread3(iy) << 1) | spread3(iz);
@@ -113,17 +127,29 @@ __device__ void finalize_norm(Scalars *sc, const double com[3], double vcen[3]) 
   }
 }
 
-__global__ void finalize_kernel(const double *__restrict__ partials, int nparts, double amp,
-                                int L, Scalars *sc) {
-  if (threadIdx.x != 0) return;
-  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  double sm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-  for (int b = 0; b < nparts; ++b) {
-    const double *q = partials + 10 * b;
-    for (int k = 0; k < 3; ++k) { mn[k] = fmin(mn[k], q[k]); mx[k] = fmax(mx[k], q[3 + k]); }
-    sm = __dadd_rn(sm, q[6]);
-    sx = __dadd_rn(sx, q[7]); sy = __dadd_rn(sy, q[8]); sz = __dadd_rn(sz, q[9]);
+// One warp per reduced quantity, fixed lane strides and a fixed butterfly:
+// deterministic.  Thread 0 then derives ssa, the centre of mass, the
+// normalised box centre and the key margin.
+__global__ void __launch_bounds__(320)
+finalize_kernel(const double *__restrict__ partials, int nparts, double amp, int L, Scalars *sc) {
+  __shared__ double red[10];
+  const int w = threadIdx.x / kWarp, lane = threadIdx.x & (kWarp - 1);
+  if (w < 10) {
+    double acc = w < 3 ? INFINITY : (w < 6 ? -INFINITY : 0.0);
+    for (int b = lane; b < nparts; b += kWarp) {
+      const double v = partials[10 * b + w];
+      acc = w < 3 ? fmin(acc, v) : (w < 6 ? fmax(acc, v) : __dadd_rn(acc, v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v = __shfl_xor_sync(0xffffffffu, acc, o);
+      acc = w < 3 ? fmin(acc, v) : (w < 6 ? fmax(acc, v) : __dadd_rn(acc, v));
+    }
+    if (lane == 0) red[w] = acc;
   }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double mn[3] = {red[0], red[1], red[2]}, mx[3] = {red[3], red[4], red[5]};
+  const double sm = red[6], sx = red[7], sy = red[8], sz = red[9];
   for (int k = 0; k < 3; ++k) { sc->bmin[k] = mn[k]; sc->bmax[k] = mx[k]; }
   double ext = __dsub_rn(mx[0], mn[0]);
   double ey = __dsub_rn(mx[1], mn[1]), ez = __dsub_rn(mx[2], mn[2]);
@@ -137,33 +163,46 @@ __global__ void finalize_kernel(const double *__restrict__ partials, int nparts,
   sc->L = L;
   sc->err = 0;
   sc->key_mismatch = 0;
+  sc->key_ambiguous = 0;
   bool ok = isfinite(sm) && sm > 0.0 && isfinite(sc->com[0]) && isfinite(sc->com[1]) &&
             isfinite(sc->com[2]) && isfinite(ext) && ext > 0.0;
   if (!ok) sc->err |= kErrNonFinite;
   finalize_norm(sc, sc->com, sc->vcen);
+  // V = largest |normalised coordinate| before the shift
+  double V = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    V = fmax(V, fabs((sc->bmin[k] - sc->com[k]) / sc->ssa));
+    V = fmax(V, fabs((sc->bmax[k] - sc->com[k]) / sc->ssa));
+  }
+  // 2 evaluations x (6.02 V + 1.5) u, x 1.5 safety, in units of 2^-21
+  sc->key_margin = 3.0 * (6.1 * V + 1.6) * ldexp(1.0, -32);
 }
 
 __global__ void __launch_bounds__(256)
 keys_kernel(const double *__restrict__ x, const double *__restrict__ y,
-            const double *__restrict__ z, int64_t n, int L, const Scalars *__restrict__ sc,
+            const double *__restrict__ z, int64_t n, int L, Scalars *sc,
             uint64_t *__restrict__ keys, int32_t *__restrict__ vals, int *err) {
   const double com[3] = {sc->com[0], sc->com[1], sc->com[2]};
   const double vcen[3] = {sc->vcen[0], sc->vcen[1], sc->vcen[2]};
   const double ssa = sc->ssa;
-  int bad = 0;
+  const double margin = sc->key_margin;
+  int bad = 0, amb = 0;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t k = key_of(x[p], y[p], z[p], com, ssa, vcen, kMaxDepth, &bad);
+    uint64_t k = key_of(x[p], y[p], z[p], com, ssa, vcen, kMaxDepth, &bad, margin, &amb);
     keys[p] = (L == kMaxDepth || L == 0) ? k : (k >> (3 * (kMaxDepth - L)));
     vals[p] = (int32_t)p;
   }
   if (bad) atomicOr(err, kErrNonFinite);
+  if (amb) atomicOr(&sc->key_ambiguous, 1);
 }
 
 // Sequential centre of mass in the reference's order (morton_octree.f90:364-370):
-// qcm = qcm + m_p q_p, mass = mass + m_p for p = 1..N.  Warps 1..7 stage the
-// next tile into shared memory while warp 0 folds the current tile; all lanes
-// of warp 0 run the same chain (broadcast reads), so there is no divergence.
+// qcm = qcm + m_p q_p, mass = mass + m_p for p = 1..N, one dependent chain per
+// component.  Warps 0..3 each fold one chain (x, y, z, mass) over the current
+// shared-memory tile, all lanes of a warp running the same chain on broadcast
+// reads, while warps 4..7 stage the next tile.  Only needed when a body lies
+// within the rounding margin of a cell edge (see the file comment).
 constexpr int kSeqTile = 1024;
 constexpr int kSeqThreads = 256;
 
@@ -172,12 +211,13 @@ seq_com_kernel(const double *__restrict__ m, const double *__restrict__ x,
                const double *__restrict__ y, const double *__restrict__ z, int64_t n,
                int com_mode, Scalars *sc) {
   extern __shared__ double4 tile[];  // 2 x kSeqTile entries: (m, x, y, z)
+  __shared__ double res[4];
   const int warp = threadIdx.x / kWarp;
   const int64_t ntiles = (n + kSeqTile - 1) / kSeqTile;
-  double ax = 0.0, ay = 0.0, az = 0.0, am = 0.0;
+  double acc = 0.0;
   auto stage = [&](int64_t t, int buf) {
-    if (warp == 0) return;
-    for (int i = threadIdx.x - kWarp; i < kSeqTile; i += kSeqThreads - kWarp) {
+    if (warp < 4) return;
+    for (int i = threadIdx.x - 4 * kWarp; i < kSeqTile; i += kSeqThreads - 4 * kWarp) {
       int64_t p = t * kSeqTile + i;
       double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
       if (p < n) v = make_double4(m[p], x[p], y[p], z[p]);
@@ -187,38 +227,31 @@ seq_com_kernel(const double *__restrict__ m, const double *__restrict__ x,
   stage(0, 0);
   __syncthreads();
   for (int64_t t = 0; t < ntiles; ++t) {
-    int buf = (int)(t & 1);
+    const int buf = (int)(t & 1);
     if (t + 1 < ntiles) stage(t + 1, buf ^ 1);
-    if (warp == 0) {
-      int cnt = (int)bh_min64(kSeqTile, n - t * kSeqTile);
-      const double4 *q = tile + buf * kSeqTile;
-      if (com_mode) {
-#pragma unroll 8
-        for (int i = 0; i < cnt; ++i) {
-          double4 v = q[i];
-          ax = __fma_rn(v.x, v.y, ax);
-          ay = __fma_rn(v.x, v.z, ay);
-          az = __fma_rn(v.x, v.w, az);
-          am = __dadd_rn(am, v.x);
-        }
+    if (warp < 4) {
+      const int cnt = (int)bh_min64(kSeqTile, n - t * kSeqTile);
+      const double *q = reinterpret_cast<const double *>(tile + buf * kSeqTile);
+      if (warp == 3) {
+#pragma unroll 16
+        for (int i = 0; i < cnt; ++i) acc = __dadd_rn(acc, q[4 * i]);
+      } else if (com_mode) {
+#pragma unroll 16
+        for (int i = 0; i < cnt; ++i) acc = __fma_rn(q[4 * i], q[4 * i + 1 + warp], acc);
       } else {
-#pragma unroll 8
-        for (int i = 0; i < cnt; ++i) {
-          double4 v = q[i];
-          ax = __dadd_rn(ax, __dmul_rn(v.x, v.y));
-          ay = __dadd_rn(ay, __dmul_rn(v.x, v.z));
-          az = __dadd_rn(az, __dmul_rn(v.x, v.w));
-          am = __dadd_rn(am, v.x);
-        }
+#pragma unroll 16
+        for (int i = 0; i < cnt; ++i) acc = __dadd_rn(acc, __dmul_rn(q[4 * i], q[4 * i + 1 + warp]));
       }
     }
     __syncthreads();
   }
+  if (warp < 4 && (threadIdx.x & (kWarp - 1)) == 0) res[warp] = acc;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    sc->mass_seq = am;
-    sc->com_seq[0] = __ddiv_rn(ax, am);
-    sc->com_seq[1] = __ddiv_rn(ay, am);
-    sc->com_seq[2] = __ddiv_rn(az, am);
+    sc->mass_seq = res[3];
+    sc->com_seq[0] = __ddiv_rn(res[0], res[3]);
+    sc->com_seq[1] = __ddiv_rn(res[1], res[3]);
+    sc->com_seq[2] = __ddiv_rn(res[2], res[3]);
   }
 }
 
@@ -297,24 +330,17 @@ __global__ void apply_depth_kernel(uint64_t *__restrict__ k, int64_t n, Scalars 
 }  // namespace
 
 void launch_keys(const double *m, const double *x, const double *y, const double *z, int64_t n,
-                 int L, double amp, int com_mode, int strict, Buffers &b, cudaStream_t s,
-                 cudaStream_t side, cudaEvent_t side_done) {
+                 int L, double amp, int com_mode, Buffers &b, cudaStream_t s) {
   reduce_partials<<<kRedBlocks, kRedThreads, 0, s>>>(m, x, y, z, n, com_mode, b.partials);
-  finalize_kernel<<<1, 32, 0, s>>>(b.partials, kRedBlocks, amp, L == 0 ? kMaxDepth : L, b.sc);
-  if (strict && side) {
-    // the side stream must see the inputs: it is ordered after everything
-    // already queued on s by the caller through an event recorded there
-    cudaEvent_t ready;
-    cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
-    cudaEventRecord(ready, s);
-    cudaStreamWaitEvent(side, ready, 0);
-    cudaEventDestroy(ready);
-    size_t smem = 2 * kSeqTile * sizeof(double4);
-    seq_com_kernel<<<1, kSeqThreads, smem, side>>>(m, x, y, z, n, com_mode, b.sc);
-    cudaEventRecord(side_done, side);
-  }
+  finalize_kernel<<<1, 320, 0, s>>>(b.partials, kRedBlocks, amp, L == 0 ? kMaxDepth : L, b.sc);
   keys_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(x, y, z, n, L == 0 ? kMaxDepth : L, b.sc,
                                                          b.k0, b.v0, &b.sc->err);
+}
+
+// The reference's sequential centre of mass (slow path, ambiguous keys only).
+void launch_seq_com(const double *m, const double *x, const double *y, const double *z,
+                    int64_t n, int com_mode, Buffers &b, cudaStream_t s) {
+  seq_com_kernel<<<1, kSeqThreads, 2 * kSeqTile * sizeof(double4), s>>>(m, x, y, z, n, com_mode, b.sc);
 }
 
 // Keys from the centre of mass already in the scalars (rebuild path).

@@ -114,8 +114,15 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
   return x - v;
 }
 
-// Stage one cell (node j) as T words: rel x, y, z, mass, then quadrupole
-// (xx yy zz xy xz yz tr), then octupole (O1..O10, O12, O13, O14).
+// Stage one cell (node j) as T words, all in the group's frame (positions
+// relative to the group centre over the root cube side, masses over the total
+// mass):
+//   [0..3]   x, y, z, m
+//   [4..7]   7.5 Qxx, 7.5 Qyy, 7.5 Qzz, 7.5 Qxy
+//   [8..11]  7.5 Qxz, 7.5 Qyz, -1.5 trQ, O14
+//   [12..23] O1..O10, O12, O13     (octupole only)
+// The factors 7.5 and -1.5 of the reference's cell formula
+// (octree_default.f90:2024-2027) are folded in here once per staged cell.
 template <typename T, int ORDER>
 __device__ __forceinline__ void stage_cell(T *w, int j, const WalkArgs &a, const double gc[3],
                                            double inv_s, double inv_m, double nq, double no) {
@@ -127,20 +134,21 @@ __device__ __forceinline__ void stage_cell(T *w, int j, const WalkArgs &a, const
   if (ORDER >= 4) {
     if (sizeof(T) == 4) {
       const float4 q0 = a.fq[2 * (int64_t)j], q1 = a.fq[2 * (int64_t)j + 1];
-      w[4] = (T)q0.x; w[5] = (T)q0.y; w[6] = (T)q0.z; w[7] = (T)q0.w;
-      w[8] = (T)q1.x; w[9] = (T)q1.y; w[10] = (T)q1.z;
+      w[4] = (T)(7.5f * q0.x); w[5] = (T)(7.5f * q0.y); w[6] = (T)(7.5f * q0.z); w[7] = (T)(7.5f * q0.w);
+      w[8] = (T)(7.5f * q1.x); w[9] = (T)(7.5f * q1.y); w[10] = (T)(-1.5f * q1.z);
     } else {
       const double *q = a.quad + 6 * (int64_t)j;
-      double q0 = q[0] * nq, q1 = q[1] * nq, q2 = q[2] * nq;
-      w[4] = (T)q0; w[5] = (T)q1; w[6] = (T)q2;
-      w[7] = (T)(q[3] * nq); w[8] = (T)(q[4] * nq); w[9] = (T)(q[5] * nq);
-      w[10] = (T)(q0 + q1 + q2);
+      const double q0 = q[0] * nq, q1 = q[1] * nq, q2 = q[2] * nq;
+      w[4] = (T)(7.5 * q0); w[5] = (T)(7.5 * q1); w[6] = (T)(7.5 * q2);
+      w[7] = (T)(7.5 * q[3] * nq); w[8] = (T)(7.5 * q[4] * nq); w[9] = (T)(7.5 * q[5] * nq);
+      w[10] = (T)(-1.5 * (q0 + q1 + q2));
     }
+    w[11] = (T)0;
   }
   if (ORDER >= 8) {
     if (sizeof(T) == 4) {
       const float4 *f = a.fo + 4 * (int64_t)j;
-      float4 o0 = f[0], o1 = f[1], o2 = f[2], o3 = f[3];
+      const float4 o0 = f[0], o1 = f[1], o2 = f[2], o3 = f[3];
       w[12] = (T)o0.x; w[13] = (T)o0.y; w[14] = (T)o0.z; w[15] = (T)o0.w;
       w[16] = (T)o1.x; w[17] = (T)o1.y; w[18] = (T)o1.z; w[19] = (T)o1.w;
       w[20] = (T)o2.x; w[21] = (T)o2.y; w[22] = (T)o2.z; w[23] = (T)o2.w;
@@ -155,14 +163,54 @@ __device__ __forceinline__ void stage_cell(T *w, int j, const WalkArgs &a, const
   }
 }
 
-// One cell interaction, accumulated into (bx, by, bz); returns nothing.
-// r^-3 is factored out of every term (see file comment).
+// Vector loads of W staged words (float4 / double2).
+template <int W>
+__device__ __forceinline__ void load_words(const float *p, float (&w)[W]) {
+#pragma unroll
+  for (int k = 0; k < W; k += 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(p + k);
+    w[k] = v.x; w[k + 1] = v.y; w[k + 2] = v.z; w[k + 3] = v.w;
+  }
+}
+template <int W>
+__device__ __forceinline__ void load_words(const double *p, double (&w)[W]) {
+#pragma unroll
+  for (int k = 0; k < W; k += 2) {
+    const double2 v = *reinterpret_cast<const double2 *>(p + k);
+    w[k] = v.x; w[k + 1] = v.y;
+  }
+}
+
+// Smallest r^2 of a body pair when there is no softening: a body meets itself
+// (d = 0, contribution exactly 0) and exactly coincident bodies contribute 0;
+// r^-3 stays finite in T.
+template <typename T> __device__ __forceinline__ T r2_floor();
+template <> __device__ __forceinline__ float r2_floor<float>() { return 1e-24f; }
+template <> __device__ __forceinline__ double r2_floor<double>() { return 1e-200; }
+
+// One body-body term added to (bx, by, bz) (morton_octree.f90:676-686).
+template <typename T, bool SOFT>
+__device__ __forceinline__ void body_force(T sx, T sy, T sz, T sm, T rx, T ry, T rz, T eps2,
+                                           T &bx, T &by, T &bz) {
+  const T dx = sx - rx, dy = sy - ry, dz = sz - rz;
+  T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
+  if (!SOFT) r2 = max(r2, r2_floor<T>());
+  const T ri = rsqrt(r2);
+  const T f = (sm * ri) * (ri * ri);
+  bx = fma(f, dx, bx); by = fma(f, dy, by); bz = fma(f, dz, bz);
+}
+
+// One cell term added to (bx, by, bz): the reference's grouped-walk formula
+// (octree_default.f90:1993-2083) with r^-3 factored out of every term:
+//   a += r^-3 [ (M - 1.5 trQ r^-2 + 7.5 dQd r^-4) d - 3 r^-2 Q d + r^3 O(d) ].
+// Accepted cells never coincide with a target (the group box lies outside the
+// MAC radius), so r^2 > 0.
 template <typename T, int ORDER>
 __device__ __forceinline__ void cell_force(const T *w, T rx, T ry, T rz, T eps2, T &bx, T &by,
                                            T &bz) {
   const T dx = w[0] - rx, dy = w[1] - ry, dz = w[2] - rz;
   const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-  const T rinv = Ops<T>::rsq(r2);
+  const T rinv = rsqrt(r2);
   const T r2i = rinv * rinv;
   const T r3i = rinv * r2i;
   if (ORDER < 4) {
@@ -170,58 +218,282 @@ __device__ __forceinline__ void cell_force(const T *w, T rx, T ry, T rz, T eps2,
     bx = fma(f, dx, bx); by = fma(f, dy, by); bz = fma(f, dz, bz);
     return;
   }
-  const T qxx = w[4], qyy = w[5], qzz = w[6], qxy = w[7], qxz = w[8], qyz = w[9], tr = w[10];
-  const T qx = fma(qxx, dx, fma(qxy, dy, qxz * dz));
-  const T qy = fma(qxy, dx, fma(qyy, dy, qyz * dz));
-  const T qz = fma(qxz, dx, fma(qyz, dy, qzz * dz));
-  const T dqd = fma(dx, qx, fma(dy, qy, dz * qz));
-  // r^3 s = M - 1.5 tr r^-2 + 7.5 dQd r^-4
-  const T A = fma((T)7.5 * dqd, r2i * r2i, fma((T)-1.5 * tr, r2i, w[3]));
-  const T m3 = (T)-3.0 * r2i;
-  T fx = fma(A, dx, m3 * qx), fy = fma(A, dy, m3 * qy), fz = fma(A, dz, m3 * qz);
-  if (ORDER >= 8) {
-    const T O1 = w[12], O2 = w[13], O3 = w[14], O4 = w[15], O5 = w[16], O6 = w[17], O7 = w[18],
-            O8 = w[19], O9 = w[20], O10 = w[21], O12 = w[22], O13 = w[23], O14 = w[11];
-    const T s7 = (T)7.5 * r2i * r2i;   // 7.5 r^-4
-    const T s5 = (T)-1.5 * r2i;        // -1.5 r^-2
-    const T s9 = (T)-17.5 * r2i * r2i * r2i;  // -17.5 r^-6
-    const T xx = dx * dx, yy = dy * dy, zz = dz * dz, xy = dx * dy, xz = dx * dz, yz = dy * dz;
-    const T oc = s7 * fma(dx, O12, fma(dy, O13, dz * O14));
-    T ox = fma(s5, O12, dx * oc), oy = fma(s5, O13, dy * oc), oz = fma(s5, O14, dz * oc);
-    ox = fma(s7, fma(xx, O1, fma(yy, O2, zz * O3)) + (T)2 * fma(xy, O4, fma(xz, O7, yz * O10)), ox);
-    oy = fma(s7, fma(xx, O4, fma(yy, O5, zz * O6)) + (T)2 * fma(xy, O2, fma(xz, O10, yz * O8)), oy);
-    oz = fma(s7, fma(xx, O7, fma(yy, O8, zz * O9)) + (T)2 * fma(xy, O10, fma(xz, O3, yz * O6)), oz);
-    T c3 = fma(xx * dx, O1, fma(yy * dy, O5, zz * dz * O9));
-    c3 = fma((T)3, fma(xx * dy, O4, fma(xx * dz, O7, xy * dy * O2)), c3);
-    c3 = fma((T)3, fma(yy * dz, O8, fma(xz * dz, O3, yz * dz * O6)), c3);
-    c3 = fma((T)6 * xy, dz * O10, c3);
-    c3 = s9 * c3;
-    fx += fma(dx, c3, ox); fy += fma(dy, c3, oy); fz += fma(dz, c3, oz);
+  // w[4..9] = 7.5 Q, w[10] = -1.5 trQ
+  const T qx = fma(w[4], dx, fma(w[7], dy, w[8] * dz));
+  const T qy = fma(w[7], dx, fma(w[5], dy, w[9] * dz));
+  const T qz = fma(w[8], dx, fma(w[9], dy, w[6] * dz));
+  const T dqd = fma(dx, qx, fma(dy, qy, dz * qz));          // 7.5 dQd
+  const T A = fma(dqd, r2i * r2i, fma(w[10], r2i, w[3]));  // M - 1.5 tr r^-2 + 7.5 dQd r^-4
+  const T sA = r3i * A;
+  const T t = (T)-0.4 * (r3i * r2i);                        // -3 r^-5 / 7.5
+  if (ORDER < 8) {
+    bx = fma(sA, dx, fma(t, qx, bx));
+    by = fma(sA, dy, fma(t, qy, by));
+    bz = fma(sA, dz, fma(t, qz, bz));
+    return;
   }
-  bx = fma(r3i, fx, bx); by = fma(r3i, fy, by); bz = fma(r3i, fz, bz);
+  const T O1 = w[12], O2 = w[13], O3 = w[14], O4 = w[15], O5 = w[16], O6 = w[17], O7 = w[18],
+          O8 = w[19], O9 = w[20], O10 = w[21], O12 = w[22], O13 = w[23], O14 = w[11];
+  const T s7 = (T)7.5 * r2i * r2i;          // 7.5 r^-4
+  const T s5 = (T)-1.5 * r2i;               // -1.5 r^-2
+  const T s9 = (T)-17.5 * r2i * r2i * r2i;  // -17.5 r^-6
+  const T xx = dx * dx, yy = dy * dy, zz = dz * dz, xy = dx * dy, xz = dx * dz, yz = dy * dz;
+  const T oc = s7 * fma(dx, O12, fma(dy, O13, dz * O14));
+  T ox = fma(s5, O12, dx * oc), oy = fma(s5, O13, dy * oc), oz = fma(s5, O14, dz * oc);
+  ox = fma(s7, fma(xx, O1, fma(yy, O2, zz * O3)) + (T)2 * fma(xy, O4, fma(xz, O7, yz * O10)), ox);
+  oy = fma(s7, fma(xx, O4, fma(yy, O5, zz * O6)) + (T)2 * fma(xy, O2, fma(xz, O10, yz * O8)), oy);
+  oz = fma(s7, fma(xx, O7, fma(yy, O8, zz * O9)) + (T)2 * fma(xy, O10, fma(xz, O3, yz * O6)), oz);
+  T c3 = fma(xx * dx, O1, fma(yy * dy, O5, zz * dz * O9));
+  c3 = fma((T)3, fma(xx * dy, O4, fma(xx * dz, O7, xy * dy * O2)), c3);
+  c3 = fma((T)3, fma(yy * dz, O8, fma(xz * dz, O3, yz * dz * O6)), c3);
+  c3 = fma((T)6 * xy, dz * O10, c3);
+  c3 = s9 * c3;
+  ox = fma(dx, c3, ox); oy = fma(dy, c3, oy); oz = fma(dz, c3, oz);
+  bx = fma(sA, dx, fma(t, qx, fma(r3i, ox, bx)));
+  by = fma(sA, dy, fma(t, qy, fma(r3i, oy, by)));
+  bz = fma(sA, dz, fma(t, qz, fma(r3i, oz, bz)));
 }
 
-template <typename T, int ORDER, int TPL>
+struct WalkCounters {
+  unsigned long long pp = 0, pc = 0, tests = 0;
+  int err = 0;
+};
+
+// One group: TPL targets per lane (the group has <= 32 * TPL bodies).
+template <typename T, int ORDER, int TPL, bool SOFT>
+__device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER> &S,
+                                           int32_t *stack, int stack_cap, int gf, int gn,
+                                           double inv_s, double inv_m, double nq, double no,
+                                           T eps2, T theta2, WalkCounters &wc) {
+  constexpr int W = StageWords<ORDER>::value;
+  constexpr bool kKahan = sizeof(T) == 4;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned lt = (1u << lane) - 1u;
+
+  double px[TPL], py[TPL], pz[TPL];
+  bool valid[TPL];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    const int k = lane + kWarp * t;
+    valid[t] = k < gn;
+    const double4 p = a.spos[gf + (valid[t] ? k : 0)];
+    px[t] = p.x; py[t] = p.y; pz[t] = p.z;
+  }
+  double lo[3] = {px[0], py[0], pz[0]}, hi[3] = {px[0], py[0], pz[0]};
+#pragma unroll
+  for (int t = 1; t < TPL; ++t) {
+    lo[0] = fmin(lo[0], px[t]); hi[0] = fmax(hi[0], px[t]);
+    lo[1] = fmin(lo[1], py[t]); hi[1] = fmax(hi[1], py[t]);
+    lo[2] = fmin(lo[2], pz[t]); hi[2] = fmax(hi[2], pz[t]);
+  }
+  double gc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) gc[k] = 0.5 * (warp_min(lo[k]) + warp_max(hi[k]));
+  T rx[TPL], ry[TPL], rz[TPL];
+  T ax[TPL], ay[TPL], az[TPL], cx[TPL], cy[TPL], cz[TPL];
+  T blo[3], bhi[3];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    rx[t] = (T)((px[t] - gc[0]) * inv_s);
+    ry[t] = (T)((py[t] - gc[1]) * inv_s);
+    rz[t] = (T)((pz[t] - gc[2]) * inv_s);
+    ax[t] = ay[t] = az[t] = cx[t] = cy[t] = cz[t] = (T)0;
+    if (t == 0) { blo[0] = bhi[0] = rx[0]; blo[1] = bhi[1] = ry[0]; blo[2] = bhi[2] = rz[0]; }
+    else {
+      blo[0] = min(blo[0], rx[t]); bhi[0] = max(bhi[0], rx[t]);
+      blo[1] = min(blo[1], ry[t]); bhi[1] = max(bhi[1], ry[t]);
+      blo[2] = min(blo[2], rz[t]); bhi[2] = max(bhi[2], rz[t]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { blo[k] = warp_min(blo[k]); bhi[k] = warp_max(bhi[k]); }
+
+  auto accumulate = [&](const T (&bx)[TPL], const T (&by)[TPL], const T (&bz)[TPL]) {
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) {
+      if (kKahan) {
+        kahan_add(ax[t], cx[t], bx[t]); kahan_add(ay[t], cy[t], by[t]); kahan_add(az[t], cz[t], bz[t]);
+      } else {
+        ax[t] += bx[t]; ay[t] += by[t]; az[t] += bz[t];
+      }
+    }
+  };
+  // evaluate the nb queue entries ending at position `end`
+  auto eval_bodies = [&](int end, int nb) {
+    if (lane < nb) {
+      const int p = S.bodyq[end - nb + lane];
+      const double4 s = a.spos[p];
+      T *w = S.stage + lane * 4;
+      w[0] = (T)((s.x - gc[0]) * inv_s);
+      w[1] = (T)((s.y - gc[1]) * inv_s);
+      w[2] = (T)((s.z - gc[2]) * inv_s);
+      w[3] = (T)(s.w * inv_m);
+    }
+    __syncwarp();
+    T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+#pragma unroll 2
+    for (int j = 0; j < nb; ++j) {
+      T w[4];
+      load_words<4>(S.stage + j * 4, w);
+#pragma unroll
+      for (int t = 0; t < TPL; ++t)
+        body_force<T, SOFT>(w[0], w[1], w[2], w[3], rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+    }
+    accumulate(bx, by, bz);
+    wc.pp += (unsigned long long)nb * gn;
+    __syncwarp();
+  };
+  auto eval_cells = [&](int end, int nc) {
+    if (lane < nc)
+      stage_cell<T, ORDER>(S.stage + lane * W, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
+    __syncwarp();
+    T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+#pragma unroll 2
+    for (int j = 0; j < nc; ++j) {
+      T w[W];
+      load_words<W>(S.stage + j * W, w);
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) cell_force<T, ORDER>(w, rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+    }
+    accumulate(bx, by, bz);
+    wc.pc += (unsigned long long)nc * gn;
+    __syncwarp();
+  };
+
+  int top = 1, ncell = 0, nbody = 0;
+  // a tree visits every node at most once per group: more tests than nodes
+  // means a malformed tree, and the walk stops with an error instead of
+  // looping
+  const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
+  int64_t group_tests = 0;
+  if (lane == 0) stack[0] = 0;
+  __syncwarp();
+  while (top > 0) {
+    if (group_tests > max_tests) { wc.err |= kErrIndex; break; }
+    const int take = min(top, kWarp);
+    const int base = top - take;
+    const int node = lane < take ? stack[base + lane] : -1;
+    top = base;
+    __syncwarp();
+    int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
+    int4 mt = make_int4(0, 0, 0, 0);
+    if (node >= 0) {
+      mt = a.meta[node];
+      const double4 c = a.com[node];
+      const T dx = (T)((c.x - gc[0]) * inv_s), dy = (T)((c.y - gc[1]) * inv_s),
+              dz = (T)((c.z - gc[2]) * inv_s);
+      const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
+      const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
+      const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
+      const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
+      const T size2 = (T)ldexp(1.0, -2 * mt.z);
+      if (size2 <= theta2 * d2) cls = 1;
+      else if (mt.y <= a.leaf_cap || mt.w == 0) cls = 2;
+      else cls = 3;
+    }
+    wc.tests += take;
+    group_tests += take;
+    // cells
+    const unsigned cm = __ballot_sync(kFull, cls == 1);
+    if (cls == 1) S.cellq[ncell + __popc(cm & lt)] = node;
+    ncell += __popc(cm);
+    // children of opened internal nodes
+    int32_t ch[8];
+    int nnc = 0, npc = 0;
+    if (cls == 3) {
+      const int4 *cp = reinterpret_cast<const int4 *>(a.child + 8 * (int64_t)node);
+      const int4 c0 = cp[0], c1 = cp[1];
+      ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
+      ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < mt.w) { if (ch[c] >= 0) ++nnc; else ++npc; }
+    }
+    int tot;
+    const int soff = warp_excl_scan(nnc, lane, tot);
+    if (top + tot > stack_cap) {
+      // capacity exceeded: the group's result is incomplete and flagged;
+      // the host repeats the walk with a larger stack
+      wc.err |= kErrStackOverflow;
+    } else {
+      if (cls == 3) {
+        int k = top + soff;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < mt.w && ch[c] >= 0) stack[k++] = ch[c];
+      }
+      top += tot;
+    }
+    // bodies: lone-particle children (<= 8, one pass) and leaf ranges
+    int rf = 0, rn = 0;
+    if (cls == 2) { rf = mt.x; rn = mt.y; }
+    bool first_pass = true;
+    for (;;) {
+      int give;
+      if (first_pass && cls == 3) give = npc;
+      else give = min(rn, kBodyPerLane);
+      int btot;
+      const int boff = warp_excl_scan(give, lane, btot);
+      if (btot == 0) break;
+      if (first_pass && cls == 3) {
+        int k = nbody + boff;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < mt.w && ch[c] < 0) S.bodyq[k++] = ~ch[c];
+      } else {
+        for (int k = 0; k < give; ++k) S.bodyq[nbody + boff + k] = rf + k;
+        rf += give; rn -= give;
+      }
+      first_pass = false;
+      nbody += btot;
+      __syncwarp();
+      while (nbody >= kWarp) { eval_bodies(nbody, kWarp); nbody -= kWarp; }
+    }
+    __syncwarp();
+    while (ncell >= kWarp) { eval_cells(ncell, kWarp); ncell -= kWarp; }
+    __syncwarp();
+  }
+  if (ncell > 0) eval_cells(ncell, ncell);
+  if (nbody > 0) eval_bodies(nbody, nbody);
+
+  // forces in the original order
+  const double scale = a.G * a.sc->mass * inv_s * inv_s;
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    if (!valid[t]) continue;
+    const int i = gf + lane + kWarp * t;
+    const int p = a.perm[i];
+    double fxs = (double)ax[t], fys = (double)ay[t], fzs = (double)az[t];
+    if (kKahan) { fxs -= (double)cx[t]; fys -= (double)cy[t]; fzs -= (double)cz[t]; }
+    double sc = scale;
+    if (a.out_kind == 0) sc *= a.spos[i].w;
+    a.out[p] = fxs * sc;
+    a.out[a.n + p] = fys * sc;
+    a.out[2 * a.n + p] = fzs * sc;
+  }
+}
+
+// Persistent warps take groups from a global cursor.  With 64-body groups a
+// group of <= 32 bodies runs the one-target-per-lane path.
+template <typename T, int ORDER, int MAXTPL, bool SOFT>
 __global__ void __launch_bounds__(kWalkWarps * kWarp)
 group_walk_kernel(WalkArgs a) {
   __shared__ WarpSmem<T, ORDER> shm[kWalkWarps];
-  constexpr int W = StageWords<ORDER>::value;
-  constexpr bool kKahan = sizeof(T) == 4;
   const int lane = threadIdx.x & (kWarp - 1), wid = threadIdx.x / kWarp;
   WarpSmem<T, ORDER> &S = shm[wid];
   const int64_t slot = (int64_t)blockIdx.x * kWalkWarps + wid;
   int32_t *stack = a.stack + slot * a.stack_cap;
   const int stack_cap = (int)a.stack_cap;
   const int ngroups = a.sc->n_groups;
-  const double ssa = a.sc->ssa, Mtot = a.sc->mass;
-  const double inv_s = 1.0 / ssa, inv_m = 1.0 / Mtot;
+  const double inv_s = 1.0 / a.sc->ssa, inv_m = 1.0 / a.sc->mass;
   const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
   const T eps2 = (T)(a.eps2 * inv_s * inv_s);
   const T theta2 = (T)a.theta2;
-  const unsigned lt = (1u << lane) - 1u;
-  int err = 0;
-  unsigned long long n_pp = 0, n_pc = 0, n_tests = 0;
-
+  WalkCounters wc;
   for (;;) {
     int g = 0;
     if (lane == 0) g = atomicAdd(a.cursor, 1);
@@ -229,229 +501,16 @@ group_walk_kernel(WalkArgs a) {
     if (g >= ngroups) break;
     const int gf = a.g_first[g];
     const int gn = a.g_first[g + 1] - gf;
-
-    double px[TPL], py[TPL], pz[TPL];
-    bool valid[TPL];
-#pragma unroll
-    for (int t = 0; t < TPL; ++t) {
-      const int k = lane + kWarp * t;
-      valid[t] = k < gn;
-      const double4 p = a.spos[gf + (valid[t] ? k : 0)];
-      px[t] = p.x; py[t] = p.y; pz[t] = p.z;
-    }
-    double lo[3] = {px[0], py[0], pz[0]}, hi[3] = {px[0], py[0], pz[0]};
-#pragma unroll
-    for (int t = 1; t < TPL; ++t) {
-      lo[0] = fmin(lo[0], px[t]); hi[0] = fmax(hi[0], px[t]);
-      lo[1] = fmin(lo[1], py[t]); hi[1] = fmax(hi[1], py[t]);
-      lo[2] = fmin(lo[2], pz[t]); hi[2] = fmax(hi[2], pz[t]);
-    }
-    double gc[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) gc[k] = 0.5 * (warp_min(lo[k]) + warp_max(hi[k]));
-    T rx[TPL], ry[TPL], rz[TPL];
-    T ax[TPL], ay[TPL], az[TPL], cx[TPL], cy[TPL], cz[TPL];
-    T blo[3], bhi[3];
-#pragma unroll
-    for (int t = 0; t < TPL; ++t) {
-      rx[t] = (T)((px[t] - gc[0]) * inv_s);
-      ry[t] = (T)((py[t] - gc[1]) * inv_s);
-      rz[t] = (T)((pz[t] - gc[2]) * inv_s);
-      ax[t] = ay[t] = az[t] = cx[t] = cy[t] = cz[t] = (T)0;
-      if (t == 0) { blo[0] = bhi[0] = rx[0]; blo[1] = bhi[1] = ry[0]; blo[2] = bhi[2] = rz[0]; }
-      else {
-        blo[0] = min(blo[0], rx[t]); bhi[0] = max(bhi[0], rx[t]);
-        blo[1] = min(blo[1], ry[t]); bhi[1] = max(bhi[1], ry[t]);
-        blo[2] = min(blo[2], rz[t]); bhi[2] = max(bhi[2], rz[t]);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) { blo[k] = warp_min(blo[k]); bhi[k] = warp_max(bhi[k]); }
-
-    // evaluate the n entries ending at queue position `end`
-    auto eval_bodies = [&](int end, int nb) {
-      if (lane < nb) {
-        const int p = S.bodyq[end - nb + lane];
-        const double4 s = a.spos[p];
-        T *w = S.stage + lane * 4;
-        w[0] = (T)((s.x - gc[0]) * inv_s);
-        w[1] = (T)((s.y - gc[1]) * inv_s);
-        w[2] = (T)((s.z - gc[2]) * inv_s);
-        w[3] = (T)(s.w * inv_m);
-      }
-      __syncwarp();
-      T bx[TPL], by[TPL], bz[TPL];
-#pragma unroll
-      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
-      for (int j = 0; j < nb; ++j) {
-        const T *w = S.stage + j * 4;
-        const T sx = w[0], sy = w[1], sz = w[2], sm = w[3];
-#pragma unroll
-        for (int t = 0; t < TPL; ++t) {
-          const T dx = sx - rx[t], dy = sy - ry[t], dz = sz - rz[t];
-          const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-          const T ri = Ops<T>::rsq(r2);
-          const T f = sm * ri * ri * ri;
-          bx[t] = fma(f, dx, bx[t]); by[t] = fma(f, dy, by[t]); bz[t] = fma(f, dz, bz[t]);
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < TPL; ++t) {
-        if (kKahan) {
-          kahan_add(ax[t], cx[t], bx[t]); kahan_add(ay[t], cy[t], by[t]); kahan_add(az[t], cz[t], bz[t]);
-        } else {
-          ax[t] += bx[t]; ay[t] += by[t]; az[t] += bz[t];
-        }
-      }
-      n_pp += (unsigned long long)nb * gn;
-      __syncwarp();
-    };
-    auto eval_cells = [&](int end, int nc) {
-      if (lane < nc) stage_cell<T, ORDER>(S.stage + lane * W, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
-      __syncwarp();
-      T bx[TPL], by[TPL], bz[TPL];
-#pragma unroll
-      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
-      for (int j = 0; j < nc; ++j) {
-        T w[W];
-#pragma unroll
-        for (int k = 0; k < W; ++k) w[k] = S.stage[j * W + k];
-#pragma unroll
-        for (int t = 0; t < TPL; ++t) cell_force<T, ORDER>(w, rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
-      }
-#pragma unroll
-      for (int t = 0; t < TPL; ++t) {
-        if (kKahan) {
-          kahan_add(ax[t], cx[t], bx[t]); kahan_add(ay[t], cy[t], by[t]); kahan_add(az[t], cz[t], bz[t]);
-        } else {
-          ax[t] += bx[t]; ay[t] += by[t]; az[t] += bz[t];
-        }
-      }
-      n_pc += (unsigned long long)nc * gn;
-      __syncwarp();
-    };
-
-    int top = 1, ncell = 0, nbody = 0;
-    // a tree visits every node at most once per group: more tests than nodes
-    // means a malformed tree, and the walk stops with an error instead of
-    // looping
-    const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
-    int64_t group_tests = 0;
-    if (lane == 0) stack[0] = 0;
-    __syncwarp();
-    while (top > 0) {
-      if (group_tests > max_tests) { err |= kErrIndex; break; }
-      const int take = min(top, kWarp);
-      const int base = top - take;
-      const int node = lane < take ? stack[base + lane] : -1;
-      top = base;
-      __syncwarp();
-      int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
-      int4 mt = make_int4(0, 0, 0, 0);
-      if (node >= 0) {
-        mt = a.meta[node];
-        const double4 c = a.com[node];
-        const T dx = (T)((c.x - gc[0]) * inv_s), dy = (T)((c.y - gc[1]) * inv_s),
-                dz = (T)((c.z - gc[2]) * inv_s);
-        const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
-        const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
-        const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
-        const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
-        const T size2 = (T)ldexp(1.0, -2 * mt.z);
-        if (size2 <= theta2 * d2) cls = 1;
-        else if (mt.y <= a.leaf_cap || mt.w == 0) cls = 2;
-        else cls = 3;
-      }
-      n_tests += take;
-      group_tests += take;
-      // cells
-      const unsigned cm = __ballot_sync(kFull, cls == 1);
-      if (cls == 1) S.cellq[ncell + __popc(cm & lt)] = node;
-      ncell += __popc(cm);
-      // children of opened internal nodes
-      int32_t ch[8];
-      int nnc = 0, npc = 0;
-      if (cls == 3) {
-        const int4 *cp = reinterpret_cast<const int4 *>(a.child + 8 * (int64_t)node);
-        const int4 c0 = cp[0], c1 = cp[1];
-        ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
-        ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < mt.w) { if (ch[c] >= 0) ++nnc; else ++npc; }
-      }
-      int tot;
-      const int soff = warp_excl_scan(nnc, lane, tot);
-      if (top + tot > stack_cap) {
-        // capacity exceeded: the group's result is incomplete and flagged;
-        // the host repeats the walk with a larger stack
-        err |= kErrStackOverflow;
-      } else {
-        if (cls == 3) {
-          int k = top + soff;
-#pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (c < mt.w && ch[c] >= 0) stack[k++] = ch[c];
-        }
-        top += tot;
-      }
-      // bodies: lone-particle children (<= 8, one pass) and leaf ranges
-      int rf = 0, rn = 0;
-      if (cls == 2) { rf = mt.x; rn = mt.y; }
-      bool first_pass = true;
-      for (;;) {
-        int give;
-        if (first_pass && cls == 3) give = npc;
-        else give = min(rn, kBodyPerLane);
-        int btot;
-        const int boff = warp_excl_scan(give, lane, btot);
-        if (btot == 0) break;
-        if (first_pass && cls == 3) {
-          int k = nbody + boff;
-#pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (c < mt.w && ch[c] < 0) S.bodyq[k++] = ~ch[c];
-        } else {
-          for (int k = 0; k < give; ++k) S.bodyq[nbody + boff + k] = rf + k;
-          rf += give; rn -= give;
-        }
-        first_pass = false;
-        nbody += btot;
-        __syncwarp();
-        while (nbody >= kWarp) { eval_bodies(nbody, kWarp); nbody -= kWarp; }
-      }
-      __syncwarp();
-      while (ncell >= kWarp) { eval_cells(ncell, kWarp); ncell -= kWarp; }
-      __syncwarp();
-    }
-    if (ncell > 0) eval_cells(ncell, ncell);
-    if (nbody > 0) eval_bodies(nbody, nbody);
-
-    // write forces in the original order
-    const double scale = a.G * Mtot * inv_s * inv_s;
-#pragma unroll
-    for (int t = 0; t < TPL; ++t) {
-      if (!valid[t]) continue;
-      const int i = gf + lane + kWarp * t;
-      const int p = a.perm[i];
-      double fxs = (double)ax[t], fys = (double)ay[t], fzs = (double)az[t];
-      if (kKahan) { fxs -= (double)cx[t]; fys -= (double)cy[t]; fzs -= (double)cz[t]; }
-      double sc = scale;
-      if (a.out_kind == 0) sc *= a.spos[i].w;
-      a.out[p] = fxs * sc;
-      a.out[a.n + p] = fys * sc;
-      a.out[2 * a.n + p] = fzs * sc;
-    }
+    if (MAXTPL == 2 && gn > kWarp)
+      walk_group<T, ORDER, 2, SOFT>(a, S, stack, stack_cap, gf, gn, inv_s, inv_m, nq, no, eps2, theta2, wc);
+    else
+      walk_group<T, ORDER, 1, SOFT>(a, S, stack, stack_cap, gf, gn, inv_s, inv_m, nq, no, eps2, theta2, wc);
   }
-  if (err && lane == 0) atomicOr(&a.sc->err, err);
-  if (a.count_stats) {
-    // per target: every body/cell batch entry interacts with each valid target
-    // of the group; counted per warp as entries x 1 and scaled on the host
-    if (lane == 0) {
-      atomicAdd(&a.stats[0], n_pp);
-      atomicAdd(&a.stats[1], n_pc);
-      atomicAdd(&a.stats[3], n_tests);
-    }
+  if (wc.err && lane == 0) atomicOr(&a.sc->err, wc.err);
+  if (a.count_stats && lane == 0) {
+    atomicAdd(&a.stats[0], wc.pp);
+    atomicAdd(&a.stats[1], wc.pc);
+    atomicAdd(&a.stats[3], wc.tests);
   }
 }
 
@@ -620,10 +679,10 @@ int64_t walk_slots() {
   return (int64_t)g_sm_count * 8 * kWalkWarps;
 }
 
-template <typename T, int ORDER, int TPL>
+template <typename T, int ORDER, int MAXTPL, bool SOFT>
 static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
   const int blocks = (int)(walk_slots() / kWalkWarps);
-  group_walk_kernel<T, ORDER, TPL><<<blocks, kWalkWarps * kWarp, 0, s>>>(a);
+  group_walk_kernel<T, ORDER, MAXTPL, SOFT><<<blocks, kWalkWarps * kWarp, 0, s>>>(a);
 }
 
 static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *out) {
@@ -637,25 +696,31 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   return a;
 }
 
+template <typename T, int ORDER>
+static void launch_walk_t(const WalkArgs &a, bool two, bool soft, cudaStream_t s) {
+  if (two) {
+    if (soft) launch_group_walk<T, ORDER, 2, true>(a, s);
+    else launch_group_walk<T, ORDER, 2, false>(a, s);
+  } else {
+    if (soft) launch_group_walk<T, ORDER, 1, true>(a, s);
+    else launch_group_walk<T, ORDER, 1, false>(a, s);
+  }
+}
+
 void launch_walk(int64_t n, const WalkParams &p, Buffers &b, double *out, cudaStream_t s) {
   WalkArgs a = make_args(n, p, b, out);
   cudaMemsetAsync(b.counters, 0, sizeof(int32_t), s);
   const bool two = p.group_size > 32;
-#define BH_WALK(T, O)                                                   \
-  do {                                                                  \
-    if (two) launch_group_walk<T, O, 2>(a, s);                          \
-    else launch_group_walk<T, O, 1>(a, s);                              \
-  } while (0)
+  const bool soft = p.eps2 > 0.0;
   if (p.precision == BH_PREC_FP64) {
-    if (p.order >= 8) BH_WALK(double, 8);
-    else if (p.order >= 4) BH_WALK(double, 4);
-    else BH_WALK(double, 1);
+    if (p.order >= 8) launch_walk_t<double, 8>(a, two, soft, s);
+    else if (p.order >= 4) launch_walk_t<double, 4>(a, two, soft, s);
+    else launch_walk_t<double, 1>(a, two, soft, s);
   } else {
-    if (p.order >= 8) BH_WALK(float, 8);
-    else if (p.order >= 4) BH_WALK(float, 4);
-    else BH_WALK(float, 1);
+    if (p.order >= 8) launch_walk_t<float, 8>(a, two, soft, s);
+    else if (p.order >= 4) launch_walk_t<float, 4>(a, two, soft, s);
+    else launch_walk_t<float, 1>(a, two, soft, s);
   }
-#undef BH_WALK
 }
 
 __global__ void inv_perm_kernel(const int32_t *__restrict__ perm, int64_t n, int32_t *__restrict__ inv) {

@@ -52,8 +52,11 @@ typedef struct bh_params {
     int leaf_cap;     /* nodes with <= leaf_cap bodies are opened into bodies (1..16) */
     int com_mode;     /* centre of mass for the keys: 0 separately rounded m*q,
                          1 fused multiply-add (what gfortran -O3 -march=native emits) */
-    int strict_keys;  /* 1: recompute the centre of mass in the reference's sequential
-                         order and re-run the build if any key differs            */
+    int strict_keys;  /* 1: keys provably equal the reference's: every body is checked
+                         against the rounding margin of its cell edges, and only if one
+                         lies inside it is the reference's sequential centre of mass
+                         computed and the build redone when a key differs;
+                         2: always run that sequential check; 0: no check          */
     int reserved[4];
 } bh_params;
 

@@ -213,3 +213,32 @@ def test_api3d_compute_forces(bh, oracle_mod):
     # accelerations
     a = api3d.compute_forces(m, x, y, z, 0.5, 1.0, 0.01, True, accelerations=True)
     np.testing.assert_allclose(a * m[:, None], f, rtol=1e-12, atol=1e-15 * np.abs(f).max())
+
+
+@pytest.mark.parametrize("strict", [1, 2])
+def test_strict_keys_repair_ambiguous_body(bh, oracle_mod, strict):
+    """tests/golden/ambiguous_keys.npz holds an input where the device's
+    parallel centre of mass and the reference's sequential one put one body in
+    different cells (made by tests/golden/make_ambiguous.py).  With strict keys
+    the device detects the body inside the rounding margin, computes the
+    sequential sum and rebuilds: keys, permutation and forces then match the
+    reference's.  Without the check the key would differ."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ambiguous_keys.npz"))
+    m, x, y, z = g["m"], g["x"], g["y"], g["z"]
+    ref = oracle_mod.MortonTree(m, x, y, z, L=21, use_quadrupole=True, fma_mode=0)
+    rkeys, rperm = ref.sorted()
+    s = bh.BHSystem()
+    f = s.forces(m, x, y, z, com_mode=0, strict_keys=strict, precision=2, theta=0.5, eps=0.01)
+    keys, perm = s.keys()
+    assert np.array_equal(keys, rkeys) and np.array_equal(perm, rperm)
+    fr = ref.forces_par(1.0, 1e-4, 0.25, True)
+    f = f.view(3, -1).T.cpu().numpy()
+    rel = np.linalg.norm(f - fr, axis=1) / np.linalg.norm(fr, axis=1)
+    assert rel.max() < 1e-9
+    s2 = bh.BHSystem()
+    s2.build(m, x, y, z, com_mode=0, strict_keys=0)
+    s2.sync()
+    k2, _ = s2.keys()
+    assert not np.array_equal(k2, rkeys), "the fast path alone should miss this body"
