@@ -34,8 +34,10 @@ EXPORTED = [
     "bh_system_create", "bh_system_destroy", "bh_system_build", "bh_system_walk",
     "bh_system_forces", "bh_system_sync", "bh_system_info", "bh_system_get_keys",
     "bh_system_get_nodes", "bh_system_get_groups", "bh_system_get_stats",
-    "bh_system_reference_targets", "bh_probe_fma_peak",
+    "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
 ]
+
+BH_NOALLOC_MAX_N = 8192
 
 
 class BHParams(C.Structure):
@@ -99,6 +101,7 @@ def lib():
             "bh_system_get_stats": [_vp, _vp],
             "bh_system_reference_targets": [_vp, C.POINTER(BHParams), _vp, _i64, _vp, _vp, _vp],
             "bh_probe_fma_peak": [_i, _vp],
+            "bh_compute_forces_noalloc": [_vp, _vp, _vp, _vp, _i64, C.POINTER(BHParams), _vp, _vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

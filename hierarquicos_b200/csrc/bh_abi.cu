@@ -19,6 +19,7 @@ struct bh_system {
   int keys_checked = 0;   // strict-key check done for the current build
   int order = 4;
   int64_t stack_cap = 4096;
+  int fixed_buffers = 0;  // buffers provided by the caller: never reallocated
   const double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
   bh_params p{};
   // the last walk of the current build, repeated if the build is redone
@@ -68,6 +69,9 @@ void free_buffers(Buffers &b) {
 int ensure_capacity(bh_system *s, int64_t n) {
   Buffers &b = s->b;
   if (b.cap >= n && b.wstack_cap >= s->stack_cap) return BH_OK;
+  if (s->fixed_buffers)
+    return set_err(BH_ERR_CAPACITY, "fixed workspace too small (n=%lld, capacity %lld)",
+                   (long long)n, (long long)b.cap);
   if (b.cap >= n) {
     // only the walk stack grows
     if (b.wstack) cudaFree(b.wstack);
@@ -194,6 +198,26 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
   w.count_stats = p->reserved[0];
   return w;
 }
+
+}  // namespace
+
+int bh_report_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+
+// A system over caller-provided buffers (the allocation-free entry point):
+// never reallocated, no pinned host mirror (reads go to `host_sc`).
+bh_system *bh::fixed_system_create(int device, const Buffers &b, Scalars *host_sc) {
+  bh_system *s = new bh_system();
+  s->device = device;
+  bh_params_default(&s->p);
+  s->b = b;
+  s->b.sc_host = host_sc;
+  s->stack_cap = b.wstack_cap;
+  s->fixed_buffers = 1;
+  bh::set_seq_com_smem_limit();
+  return s;
+}
+
+namespace {
 
 std::mutex g_default_mu;
 bh_system *g_default[64] = {nullptr};
@@ -346,7 +370,8 @@ int finish(bh_system *s, cudaStream_t st) {
     }
   }
   s->keys_checked = 1;
-  for (int attempt = 0; attempt < 4 && s->walked && (s->b.sc_host->err & bh::kErrStackOverflow);
+  for (int attempt = 0;
+       attempt < 4 && s->walked && !s->fixed_buffers && (s->b.sc_host->err & bh::kErrStackOverflow);
        ++attempt) {
     s->stack_cap *= 2;
     rc = ensure_capacity(s, s->n);

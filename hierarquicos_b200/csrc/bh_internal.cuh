@@ -83,7 +83,7 @@ struct Buffers {
   // walk
   int32_t *wstack = nullptr;
   int64_t wstack_cap = 0;   // entries per warp slot
-  int64_t wstack_slots = 0;
+  int64_t wstack_slots = 0; // warp slots: the walk launches wstack_slots / 4 blocks of 4 warps
   int32_t *counters = nullptr;   // [0] group cursor
   unsigned long long *stats = nullptr;  // interaction counters
   Scalars *sc = nullptr;
@@ -116,12 +116,16 @@ inline int grid_for(int64_t n, int threads, int cap) {
 // device (n is then an upper bound).
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
                       const int32_t *n_dev, int bits, int32_t *hist, cudaStream_t s);
-int64_t radix_hist_entries(int64_t n);
+// count table of the radix sort (256 digits x 4096-key tiles) + its scan
+// scratch, in int32 entries
+constexpr int64_t scan_tmp_entries(int64_t n) { return (n + 8191) / 8192 + 2; }
+constexpr int64_t radix_hist_entries(int64_t n) {
+  return 256 * ((n + 4095) / 4096) + 1 + scan_tmp_entries(256 * ((n + 4095) / 4096));
+}
 
 // exclusive scan of n int32 values; total written to *total (device) if given
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
                     int32_t *total, int32_t *tmp, cudaStream_t s);
-int64_t scan_tmp_entries(int64_t n);
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s);
@@ -150,4 +154,12 @@ void launch_direct(const double *m, const double *x, const double *y, const doub
                    const int64_t *targets, int64_t ntargets, double G, double eps2, int out_kind,
                    double *out, cudaStream_t s);
 
+}  // namespace bh
+
+struct bh_system;
+// bh_abi.cu: records `msg` as the calling thread's last error, returns code
+int bh_report_error(int code, const char *msg);
+namespace bh {
+// bh_abi.cu: a system whose workspace is `b` (caller-owned, never grown)
+bh_system *fixed_system_create(int device, const Buffers &b, Scalars *host_sc);
 }  // namespace bh

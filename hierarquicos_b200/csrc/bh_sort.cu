@@ -245,7 +245,8 @@ bool g_sort_attr_set = false;
 
 }  // namespace
 
-int64_t scan_tmp_entries(int64_t n) { return (n + kScanChunk - 1) / kScanChunk + 2; }
+static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256,
+              "scan_tmp_entries / radix_hist_entries in bh_internal.cuh assume these sizes");
 
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
                     int32_t *total, int32_t *tmp, cudaStream_t s) {
@@ -286,11 +287,7 @@ void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int6
   }
 }
 
-// count table + its scan scratch, in int32 entries
-int64_t radix_hist_entries(int64_t n) {
-  int64_t entries = (int64_t)kRadix * ((n + kTile - 1) / kTile);
-  return entries + 1 + scan_tmp_entries(entries);
-}
+
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s) {

@@ -83,6 +83,7 @@ struct WalkArgs {
   int32_t *cursor;
   int32_t *stack;
   int64_t stack_cap;
+  int64_t slots;
   unsigned long long *stats;
   double *out;
   int64_t n;
@@ -681,7 +682,7 @@ int64_t walk_slots() {
 
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
 static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
-  const int blocks = (int)(walk_slots() / kWalkWarps);
+  const int blocks = (int)(a.slots / kWalkWarps);
   group_walk_kernel<T, ORDER, MAXTPL, SOFT><<<blocks, kWalkWarps * kWarp, 0, s>>>(a);
 }
 
@@ -690,6 +691,7 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   a.meta = b.cn_meta; a.child = b.cn_child; a.com = b.cn_com; a.quad = b.cn_quad; a.oct = b.cn_oct;
   a.fq = b.cn_fq; a.fo = b.cn_fo; a.spos = b.spos; a.perm = b.v0; a.g_first = b.g_first;
   a.sc = b.sc; a.cursor = b.counters; a.stack = b.wstack; a.stack_cap = b.wstack_cap;
+  a.slots = b.wstack_slots;
   a.stats = b.stats; a.out = out; a.n = n;
   a.theta2 = p.theta2; a.G = p.G; a.eps2 = p.eps2;
   a.out_kind = p.out_kind; a.leaf_cap = p.leaf_cap; a.count_stats = p.count_stats;

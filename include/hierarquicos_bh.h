@@ -149,6 +149,19 @@ int bh_system_reference_targets(bh_system *sys, const bh_params *p, const int64_
                                 int64_t ntargets, double *d_out, int64_t *d_counts,
                                 void *stream);
 
+/* Allocation-free force evaluation, for callers that may not allocate device
+ * memory (their memory belongs to another allocator, a cudaMalloc would stall
+ * their time-step loop, or their host forbids it).  No counterpart in the
+ * reference.  Device inputs and output as bh_system_forces; everything else
+ * comes from one fixed device array of about 5.7 MB inside the library, so n
+ * is limited to BH_NOALLOC_MAX_N (larger n: BH_ERR_INVALID).  The first call on
+ * a device looks that array up; all calls on a device share it, so calls that
+ * overlap on the GPU race: run them one after another.  Synchronous. */
+#define BH_NOALLOC_MAX_N 8192
+int bh_compute_forces_noalloc(const double *d_m, const double *d_x, const double *d_y,
+                              const double *d_z, int64_t n, const bh_params *p, double *d_out,
+                              void *stream);
+
 /* FP32 and FP64 fused-multiply-add throughput probe (independent chains,
  * CUDA events): writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64). */
 int bh_probe_fma_peak(int device, double *gflops2);
