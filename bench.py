@@ -231,11 +231,11 @@ def run_ours(args):
                             "reference_walk_rms_rel": err_ref["rms_rel"],
                             "meets_1e-3": err["rms_rel"] <= 1e-3}
         # executed interactions of the group walk
-        p.reserved[0] = 1
+        p.count_stats = 1
         sysm.walk(p, out)
         sysm.sync()
         st = sysm.stats()
-        p.reserved[0] = 0
+        p.count_stats = 0
         peak = np.zeros(2)
         _lib.check(_lib.lib().bh_probe_fma_peak(local, peak.ctypes.data_as(__import__("ctypes").c_void_p)))
         alg_flops = n * (mean_pp * FLOPS_PP + mean_pc * FLOPS_PC[args.order])

@@ -35,6 +35,8 @@ EXPORTED = [
     "bh_system_forces", "bh_system_sync", "bh_system_info", "bh_system_get_keys",
     "bh_system_get_nodes", "bh_system_get_groups", "bh_system_get_stats",
     "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
+    "bh_system_build_batch", "bh_system_forces_batch", "bh_system_batch_info",
+    "bh_system_capture", "bh_system_replay",
 ]
 
 BH_NOALLOC_MAX_N = 8192
@@ -47,7 +49,8 @@ class BHParams(C.Structure):
         ("theta", C.c_double), ("G", C.c_double), ("eps", C.c_double),
         ("order", C.c_int), ("out_kind", C.c_int), ("depth", C.c_int), ("precision", C.c_int),
         ("amp", C.c_double), ("group_size", C.c_int), ("leaf_cap", C.c_int),
-        ("com_mode", C.c_int), ("strict_keys", C.c_int), ("reserved", C.c_int * 4),
+        ("com_mode", C.c_int), ("strict_keys", C.c_int), ("count_stats", C.c_int),
+        ("group_span", C.c_int), ("reserved", C.c_int * 2),
     ]
 
 
@@ -102,6 +105,12 @@ def lib():
             "bh_system_reference_targets": [_vp, C.POINTER(BHParams), _vp, _i64, _vp, _vp, _vp],
             "bh_probe_fma_peak": [_i, _vp],
             "bh_compute_forces_noalloc": [_vp, _vp, _vp, _vp, _i64, C.POINTER(BHParams), _vp, _vp],
+            "bh_system_build_batch": [_vp, _vp, _vp, _vp, _vp, _vp, _i, C.POINTER(BHParams), _vp],
+            "bh_system_forces_batch": [_vp, _vp, _vp, _vp, _vp, _vp, _i, C.POINTER(BHParams), _vp,
+                                       _vp],
+            "bh_system_batch_info": [_vp, _vp, _vp, _vp],
+            "bh_system_capture": [_vp, C.POINTER(BHParams), _vp],
+            "bh_system_replay": [_vp, _vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

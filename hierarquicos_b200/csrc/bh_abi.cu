@@ -1,11 +1,13 @@
 // C ABI of the force engine: workspace management, the build/walk pipeline
-// and status reporting.  See include/hierarquicos_bh.h for the contract.
+// for batches of systems, CUDA-graph capture and status reporting.  See
+// include/hierarquicos_bh.h for the contract.
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <mutex>
+#include <vector>
 
 #include "bh_internal.cuh"
 
@@ -14,7 +16,10 @@ using bh::Buffers;
 struct bh_system {
   int device = 0;
   Buffers b;
-  int64_t n = 0;
+  int64_t n = 0;                 // bodies of the current batch
+  int nsys = 0;                  // systems of the current batch
+  std::vector<int64_t> offsets;  // layout uploaded to the device (nsys + 1 entries)
+  std::vector<bh::RedItem> items_host;
   int built = 0;
   int keys_checked = 0;   // strict-key check done for the current build
   int order = 4;
@@ -26,6 +31,8 @@ struct bh_system {
   int walked = 0;
   bh_params walk_p{};
   double *walk_out = nullptr;
+  // captured build + walk of the current layout
+  cudaGraphExec_t graph = nullptr;
 };
 
 namespace {
@@ -54,62 +61,114 @@ cudaError_t dalloc(T **p, int64_t count) {
   return cudaMalloc((void **)p, (size_t)count * sizeof(T));
 }
 
-void free_buffers(Buffers &b) {
-  void *ptrs[] = {b.hm, b.hx, b.hy, b.hz, b.hout, b.k0, b.k1, b.v0, b.v1, b.hist, b.partials,
+void drop_graph(bh_system *s) {
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  s->graph = nullptr;
+}
+
+void free_body_buffers(Buffers &b) {
+  void *ptrs[] = {b.hm, b.hx, b.hy, b.hz, b.hout, b.k0, b.k1, b.v0, b.v1, b.hist, b.sys_of,
                   b.spos, b.bn_left, b.bn_right, b.bn_parent, b.bn_first, b.bn_last, b.bn_level,
                   b.bn_flag, b.bin2cn, b.cn_bin, b.cn_meta, b.cn_child, b.cn_parent, b.cn_com,
-                  b.cn_quad, b.cn_oct, b.cn_fq, b.cn_fo, b.level_begin, b.gflag, b.gscan,
-                  b.g_first, b.scan_tmp, b.wstack, b.counters, b.stats, b.sc};
+                  b.cn_quad, b.cn_oct, b.cn_fq, b.cn_fo, b.gflag, b.gscan, b.g_first, b.scan_tmp};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  b.hm = b.hx = b.hy = b.hz = b.hout = nullptr;
+  b.k0 = b.k1 = nullptr;
+  b.v0 = b.v1 = b.hist = b.sys_of = nullptr;
+  b.spos = nullptr;
+  b.bn_left = b.bn_right = b.bn_parent = b.bn_first = b.bn_last = b.bn_level = nullptr;
+  b.bn_flag = b.bin2cn = b.cn_bin = b.cn_child = b.cn_parent = nullptr;
+  b.cn_meta = nullptr;
+  b.cn_com = nullptr;
+  b.cn_quad = b.cn_oct = nullptr;
+  b.cn_fq = b.cn_fo = nullptr;
+  b.gflag = b.gscan = b.g_first = b.scan_tmp = nullptr;
+  b.cap = 0;
+}
+
+void free_buffers(Buffers &b) {
+  free_body_buffers(b);
+  void *ptrs[] = {b.partials, b.items, b.ss, b.level_begin, b.wstack, b.counters, b.stats, b.sc};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (b.sc_host) cudaFreeHost(b.sc_host);
+  if (b.ss_host) cudaFreeHost(b.ss_host);
   b = Buffers();
 }
 
-int ensure_capacity(bh_system *s, int64_t n) {
+// Workspace for n bodies in nsys systems with n_items reduction items.  Each
+// part grows on its own; growing the body arrays forces a new layout upload.
+int ensure_capacity(bh_system *s, int64_t n, int nsys, int n_items) {
   Buffers &b = s->b;
-  if (b.cap >= n && b.wstack_cap >= s->stack_cap) return BH_OK;
+  const bool body_ok = b.cap >= n;
+  const bool sys_ok = b.sys_cap >= nsys && b.items_cap >= n_items;
+  const bool stack_ok = b.wstack && b.wstack_cap >= s->stack_cap;
+  if (body_ok && sys_ok && stack_ok && b.sc) return BH_OK;
   if (s->fixed_buffers)
-    return set_err(BH_ERR_CAPACITY, "fixed workspace too small (n=%lld, capacity %lld)",
-                   (long long)n, (long long)b.cap);
-  if (b.cap >= n) {
-    // only the walk stack grows
+    return set_err(BH_ERR_CAPACITY,
+                   "fixed workspace too small (n=%lld in %d systems, capacity %lld bodies)",
+                   (long long)n, nsys, (long long)b.cap);
+  drop_graph(s);
+  if (!b.sc) {
+    BH_CUDA(dalloc(&b.level_begin, bh::kNumLevels + 2));
+    BH_CUDA(dalloc(&b.counters, 8));
+    BH_CUDA(dalloc(&b.stats, 4));
+    BH_CUDA(dalloc(&b.sc, 1));
+    BH_CUDA(cudaMallocHost((void **)&b.sc_host, sizeof(bh::Scalars)));
+    BH_CUDA(cudaMemset(b.sc, 0, sizeof(bh::Scalars)));
+    BH_CUDA(cudaMemset(b.stats, 0, 4 * sizeof(unsigned long long)));
+  }
+  if (!stack_ok) {
     if (b.wstack) cudaFree(b.wstack);
     b.wstack = nullptr;
     b.wstack_slots = bh::walk_slots();
     BH_CUDA(dalloc(&b.wstack, b.wstack_slots * s->stack_cap));
     b.wstack_cap = s->stack_cap;
-    return BH_OK;
   }
-  free_buffers(b);
-  const int64_t c = n < 2 ? 2 : n;
-  BH_CUDA(dalloc(&b.k0, c)); BH_CUDA(dalloc(&b.k1, c));
-  BH_CUDA(dalloc(&b.v0, c)); BH_CUDA(dalloc(&b.v1, c));
-  b.hist_cap = bh::radix_hist_entries(c);
-  BH_CUDA(dalloc(&b.hist, b.hist_cap));
-  BH_CUDA(dalloc(&b.partials, 296 * 10));
-  BH_CUDA(dalloc(&b.spos, c));
-  BH_CUDA(dalloc(&b.bn_left, c)); BH_CUDA(dalloc(&b.bn_right, c)); BH_CUDA(dalloc(&b.bn_parent, c));
-  BH_CUDA(dalloc(&b.bn_first, c)); BH_CUDA(dalloc(&b.bn_last, c)); BH_CUDA(dalloc(&b.bn_level, c));
-  BH_CUDA(dalloc(&b.bn_flag, c)); BH_CUDA(dalloc(&b.bin2cn, c));
-  BH_CUDA(dalloc(&b.cn_bin, c)); BH_CUDA(dalloc(&b.cn_meta, c)); BH_CUDA(dalloc(&b.cn_child, 8 * c));
-  BH_CUDA(dalloc(&b.cn_parent, c)); BH_CUDA(dalloc(&b.cn_com, c));
-  BH_CUDA(dalloc(&b.cn_quad, 6 * c)); BH_CUDA(dalloc(&b.cn_oct, 14 * c));
-  BH_CUDA(dalloc(&b.cn_fq, 2 * c)); BH_CUDA(dalloc(&b.cn_fo, 4 * c));
-  BH_CUDA(dalloc(&b.level_begin, bh::kNumLevels + 2));
-  BH_CUDA(dalloc(&b.gflag, c + 1)); BH_CUDA(dalloc(&b.gscan, c + 1)); BH_CUDA(dalloc(&b.g_first, c + 1));
-  b.scan_tmp_cap = bh::scan_tmp_entries(c + 1);
-  BH_CUDA(dalloc(&b.scan_tmp, b.scan_tmp_cap));
-  b.wstack_slots = bh::walk_slots();
-  BH_CUDA(dalloc(&b.wstack, b.wstack_slots * s->stack_cap));
-  b.wstack_cap = s->stack_cap;
-  BH_CUDA(dalloc(&b.counters, 8));
-  BH_CUDA(dalloc(&b.stats, 4));
-  BH_CUDA(dalloc(&b.sc, 1));
-  BH_CUDA(cudaMallocHost((void **)&b.sc_host, sizeof(bh::Scalars)));
-  BH_CUDA(cudaMemset(b.sc, 0, sizeof(bh::Scalars)));
-  BH_CUDA(cudaMemset(b.stats, 0, 4 * sizeof(unsigned long long)));
-  b.cap = c;
+  if (!sys_ok) {
+    if (b.ss) cudaFree(b.ss);
+    if (b.ss_host) cudaFreeHost(b.ss_host);
+    if (b.items) cudaFree(b.items);
+    if (b.partials) cudaFree(b.partials);
+    b.ss = nullptr;
+    b.ss_host = nullptr;
+    b.items = nullptr;
+    b.partials = nullptr;
+    const int sc_ = nsys > b.sys_cap ? nsys : b.sys_cap;
+    const int ic = n_items > b.items_cap ? n_items : b.items_cap;
+    BH_CUDA(dalloc(&b.ss, sc_));
+    BH_CUDA(cudaMallocHost((void **)&b.ss_host, (size_t)sc_ * sizeof(bh::SysScalars)));
+    BH_CUDA(dalloc(&b.items, ic));
+    BH_CUDA(dalloc(&b.partials, 10 * (int64_t)ic));
+    b.sys_cap = sc_;
+    b.items_cap = ic;
+    b.nsys = 0;
+    s->offsets.clear();
+  }
+  if (!body_ok) {
+    free_body_buffers(b);
+    const int64_t c = n < 2 ? 2 : n;
+    BH_CUDA(dalloc(&b.k0, c)); BH_CUDA(dalloc(&b.k1, c));
+    BH_CUDA(dalloc(&b.v0, c)); BH_CUDA(dalloc(&b.v1, c));
+    b.hist_cap = bh::radix_hist_entries(c);
+    BH_CUDA(dalloc(&b.hist, b.hist_cap));
+    BH_CUDA(dalloc(&b.sys_of, c));
+    BH_CUDA(dalloc(&b.spos, c));
+    BH_CUDA(dalloc(&b.bn_left, c)); BH_CUDA(dalloc(&b.bn_right, c)); BH_CUDA(dalloc(&b.bn_parent, c));
+    BH_CUDA(dalloc(&b.bn_first, c)); BH_CUDA(dalloc(&b.bn_last, c)); BH_CUDA(dalloc(&b.bn_level, c));
+    BH_CUDA(dalloc(&b.bn_flag, c)); BH_CUDA(dalloc(&b.bin2cn, c));
+    BH_CUDA(dalloc(&b.cn_bin, c)); BH_CUDA(dalloc(&b.cn_meta, c)); BH_CUDA(dalloc(&b.cn_child, 8 * c));
+    BH_CUDA(dalloc(&b.cn_parent, c)); BH_CUDA(dalloc(&b.cn_com, c));
+    BH_CUDA(dalloc(&b.cn_quad, 6 * c)); BH_CUDA(dalloc(&b.cn_oct, 14 * c));
+    BH_CUDA(dalloc(&b.cn_fq, 2 * c)); BH_CUDA(dalloc(&b.cn_fo, 4 * c));
+    BH_CUDA(dalloc(&b.gflag, c + 1)); BH_CUDA(dalloc(&b.gscan, c + 1)); BH_CUDA(dalloc(&b.g_first, c + 1));
+    b.scan_tmp_cap = bh::scan_tmp_entries(c + 1);
+    BH_CUDA(dalloc(&b.scan_tmp, b.scan_tmp_cap));
+    b.cap = c;
+    b.nsys = 0;
+    s->offsets.clear();
+  }
   return BH_OK;
 }
 
@@ -120,6 +179,45 @@ int ensure_host_staging(bh_system *s, int64_t n) {
   const int64_t c = b.cap;
   BH_CUDA(dalloc(&b.hm, c)); BH_CUDA(dalloc(&b.hx, c)); BH_CUDA(dalloc(&b.hy, c));
   BH_CUDA(dalloc(&b.hz, c)); BH_CUDA(dalloc(&b.hout, 3 * c));
+  return BH_OK;
+}
+
+// reduction work items: every system is cut into chunks of kRedChunk bodies
+int count_items(const int64_t *off, int nsys) {
+  int64_t k = 0;
+  for (int q = 0; q < nsys; ++q) k += (off[q + 1] - off[q] + bh::kRedChunk - 1) / bh::kRedChunk;
+  return (int)k;
+}
+
+// Uploads a batch layout (offsets, reduction items, system of every body)
+// unless it is the one already on the device.
+int set_layout(bh_system *s, const int64_t *off, int nsys, cudaStream_t st) {
+  Buffers &b = s->b;
+  if (b.nsys == nsys && (int)s->offsets.size() == nsys + 1 &&
+      memcmp(s->offsets.data(), off, (size_t)(nsys + 1) * sizeof(int64_t)) == 0)
+    return BH_OK;
+  drop_graph(s);
+  s->items_host.clear();
+  for (int q = 0; q < nsys; ++q)
+    for (int64_t a = off[q]; a < off[q + 1]; a += bh::kRedChunk)
+      s->items_host.push_back(
+          bh::RedItem{q, 0, a, a + bh::kRedChunk < off[q + 1] ? a + bh::kRedChunk : off[q + 1]});
+  for (int q = 0; q < nsys; ++q) {
+    memset(&b.ss_host[q], 0, sizeof(bh::SysScalars));
+    b.ss_host[q].off = off[q];
+    b.ss_host[q].n = off[q + 1] - off[q];
+    b.ss_host[q].root = -1;
+  }
+  BH_CUDA(cudaMemcpyAsync(b.ss, b.ss_host, (size_t)nsys * sizeof(bh::SysScalars),
+                          cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.items, s->items_host.data(),
+                          s->items_host.size() * sizeof(bh::RedItem), cudaMemcpyHostToDevice, st));
+  b.n_items = (int)s->items_host.size();
+  b.nsys = nsys;
+  bh::launch_layout(b, st);
+  // the host staging areas are reused by the next layout
+  BH_CUDA(cudaStreamSynchronize(st));
+  s->offsets.assign(off, off + nsys + 1);
   return BH_OK;
 }
 
@@ -140,13 +238,14 @@ int check_params(const bh_params *p, int64_t n) {
   if (p->out_kind != 0 && p->out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
   if (p->com_mode != 0 && p->com_mode != 1) return set_err(BH_ERR_INVALID, "com_mode must be 0 or 1");
   if (p->strict_keys < 0 || p->strict_keys > 2) return set_err(BH_ERR_INVALID, "strict_keys must be 0, 1 or 2");
+  if (p->group_span != 0 && (p->group_span < p->group_size || p->group_span > (1 << 20)))
+    return set_err(BH_ERR_INVALID, "group_span must be 0 or in [group_size, 2^20]");
   return BH_OK;
 }
 
-int status_from_device(bh_system *s, int ignore_stack) {
+int status_from_device(bh_system *s) {
   const bh::Scalars &h = *s->b.sc_host;
-  int e = h.err;
-  if (ignore_stack) e &= ~bh::kErrStackOverflow;
+  const int e = h.err;
   if (e & bh::kErrNonFinite)
     return set_err(BH_ERR_NONFINITE, "non-finite position or mass, or total mass <= 0");
   if (e & bh::kErrDuplicates)
@@ -164,11 +263,12 @@ int read_scalars(bh_system *s, cudaStream_t st) {
   return BH_OK;
 }
 
-// keys (from scratch or from the scalars' centre of mass) -> sort -> octree ->
-// multipoles -> groups
-void enqueue_build(bh_system *s, int64_t n, int keys_from_scalars, cudaStream_t st) {
+// keys (from scratch, or from the centres of mass already in the system
+// scalars) -> sort -> octree -> multipoles -> groups, for the whole batch
+void enqueue_build(bh_system *s, int keys_from_scalars, cudaStream_t st) {
   Buffers &b = s->b;
   const bh_params &p = s->p;
+  const int64_t n = s->n;
   const int L = p.depth;
   if (keys_from_scalars)
     bh::launch_keys_only(s->x, s->y, s->z, n, L, b, st);
@@ -176,13 +276,12 @@ void enqueue_build(bh_system *s, int64_t n, int keys_from_scalars, cudaStream_t 
     bh::launch_keys(s->m, s->x, s->y, s->z, n, L, p.amp, p.com_mode, b, st);
   const int bits = (L == 0) ? 3 * bh::kMaxDepth : 3 * L;
   bh::radix_sort_pairs(b.k0, b.v0, b.k1, b.v1, n, nullptr, bits, b.hist, st);
+  bh::launch_sort_by_system(n, b, st);
   if (L == 0) bh::launch_auto_depth(n, b, st);
   bh::launch_gather(s->m, s->x, s->y, s->z, n, b, st);
-  if (n >= 2) {
-    bh::launch_build_tree(n, L, b, st);
-    bh::launch_upward(n, L, p.order, b, st);
-    bh::launch_groups(n, p.group_size, b, st);
-  }
+  bh::launch_build_tree(n, L, b, st);
+  bh::launch_upward(n, L, p.order, b, st);
+  bh::launch_groups(n, p.group_size, p.group_span > 0 ? p.group_span : 2 * p.group_size, b, st);
 }
 
 bh::WalkParams walk_params(const bh_params *p, int order) {
@@ -195,29 +294,98 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
   w.precision = p->precision;
   w.group_size = p->group_size;
   w.leaf_cap = p->leaf_cap;
-  w.count_stats = p->reserved[0];
+  w.count_stats = p->count_stats;
   return w;
 }
 
-}  // namespace
-
-int bh_report_error(int code, const char *msg) { return set_err(code, "%s", msg); }
-
-// A system over caller-provided buffers (the allocation-free entry point):
-// never reallocated, no pinned host mirror (reads go to `host_sc`).
-bh_system *bh::fixed_system_create(int device, const Buffers &b, Scalars *host_sc) {
-  bh_system *s = new bh_system();
-  s->device = device;
-  bh_params_default(&s->p);
-  s->b = b;
-  s->b.sc_host = host_sc;
-  s->stack_cap = b.wstack_cap;
-  s->fixed_buffers = 1;
-  bh::set_seq_com_smem_limit();
-  return s;
+// the walk of the whole batch, enqueued without host synchronisation
+void enqueue_walk(bh_system *s, const bh_params *p, double *d_out, cudaStream_t st) {
+  const bh::WalkParams w = walk_params(p, s->order);
+  if (w.count_stats) cudaMemsetAsync(s->b.stats, 0, 4 * sizeof(unsigned long long), st);
+  if (p->precision == BH_PREC_REFERENCE)
+    bh::launch_reference_walk(s->n, w, s->b, d_out, nullptr, 0, nullptr, st);
+  else
+    bh::launch_walk(s->n, w, s->b, d_out, st);
 }
 
-namespace {
+int validate_offsets(const int64_t *off, int nsys, int64_t *total) {
+  if (!off || nsys < 1) return set_err(BH_ERR_INVALID, "a batch needs at least one system");
+  if (nsys > (1 << 24)) return set_err(BH_ERR_INVALID, "more than 2^24 systems");
+  if (off[0] != 0) return set_err(BH_ERR_INVALID, "offsets[0] must be 0");
+  for (int q = 0; q < nsys; ++q)
+    if (off[q + 1] <= off[q])
+      return set_err(BH_ERR_INVALID, "system %d is empty (offsets must increase strictly)", q);
+  *total = off[nsys];
+  return BH_OK;
+}
+
+int build_common(bh_system *s, const double *d_m, const double *d_x, const double *d_y,
+                 const double *d_z, const int64_t *off, int nsys, const bh_params *p,
+                 cudaStream_t st) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  int64_t n = 0;
+  int rc = validate_offsets(off, nsys, &n);
+  if (rc) return rc;
+  rc = check_params(p, n);
+  if (rc) return rc;
+  if (!d_m || !d_x || !d_y || !d_z) return set_err(BH_ERR_INVALID, "NULL input array");
+  if (nsys > 1 && p->depth == 0)
+    return set_err(BH_ERR_INVALID, "depth 0 (automatic) applies to a single system only");
+  BH_CUDA(cudaSetDevice(s->device));
+  rc = ensure_capacity(s, n, nsys, count_items(off, nsys));
+  if (rc) return rc;
+  rc = set_layout(s, off, nsys, st);
+  if (rc) return rc;
+  s->p = *p;
+  s->m = d_m; s->x = d_x; s->y = d_y; s->z = d_z;
+  s->n = n;
+  s->nsys = nsys;
+  s->order = p->order;
+  s->walked = 0;
+  enqueue_build(s, 0, st);
+  BH_CUDA(cudaGetLastError());
+  s->built = 1;
+  s->keys_checked = p->strict_keys ? 0 : 1;
+  return BH_OK;
+}
+
+// Completes a build + walk: strict-key check (slow path only when a body lies
+// within the rounding margin of a cell edge), stack-capacity retries, status.
+int finish(bh_system *s, cudaStream_t st) {
+  int rc = read_scalars(s, st);
+  if (rc) return rc;
+  if (!s->keys_checked && (s->b.sc_host->key_ambiguous || s->p.strict_keys == 2) &&
+      !(s->b.sc_host->err & bh::kErrNonFinite)) {
+    // the reference's sequential centre of mass decides the ambiguous keys
+    const int all = s->p.strict_keys == 2;
+    bh::launch_seq_com(s->m, s->x, s->y, s->z, s->p.com_mode, all, s->b, st);
+    bh::launch_verify_keys(s->x, s->y, s->z, s->n, all, s->b, st);
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+    if (s->b.sc_host->key_mismatch) {
+      bh::launch_adopt_seq_com(s->b, st);
+      enqueue_build(s, 1, st);
+      if (s->walked) enqueue_walk(s, &s->walk_p, s->walk_out, st);
+      BH_CUDA(cudaGetLastError());
+      rc = read_scalars(s, st);
+      if (rc) return rc;
+    }
+  }
+  s->keys_checked = 1;
+  for (int attempt = 0;
+       attempt < 4 && s->walked && !s->fixed_buffers && (s->b.sc_host->err & bh::kErrStackOverflow);
+       ++attempt) {
+    s->stack_cap *= 2;
+    rc = ensure_capacity(s, s->n, s->nsys, s->b.n_items);
+    if (rc) return rc;
+    BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
+    enqueue_walk(s, &s->walk_p, s->walk_out, st);
+    BH_CUDA(cudaGetLastError());
+    rc = read_scalars(s, st);
+    if (rc) return rc;
+  }
+  return status_from_device(s);
+}
 
 std::mutex g_default_mu;
 bh_system *g_default[64] = {nullptr};
@@ -234,7 +402,42 @@ int default_system(bh_system **out) {
   return BH_OK;
 }
 
+// copies host arrays into the default system's staging buffers
+int stage_inputs(bh_system *s, const double *m, const double *x, const double *y,
+                 const double *z, int64_t n, cudaStream_t st) {
+  const int64_t off[2] = {0, n};
+  int rc = ensure_capacity(s, n, 1, count_items(off, 1));
+  if (rc) return rc;
+  rc = ensure_host_staging(s, n);
+  if (rc) return rc;
+  Buffers &b = s->b;
+  BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  return BH_OK;
+}
+
 }  // namespace
+
+int bh_report_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+
+// A system over caller-provided buffers (the allocation-free entry point):
+// never reallocated; the host mirrors are the caller's.
+bh_system *bh::fixed_system_create(int device, const Buffers &b, Scalars *host_sc,
+                                   SysScalars *host_ss) {
+  bh_system *s = new bh_system();
+  s->device = device;
+  bh_params_default(&s->p);
+  s->b = b;
+  s->b.sc_host = host_sc;
+  s->b.ss_host = host_ss;
+  s->stack_cap = b.wstack_cap;
+  s->fixed_buffers = 1;
+  s->items_host.reserve(1);
+  bh::set_seq_com_smem_limit();
+  return s;
+}
 
 extern "C" {
 
@@ -254,7 +457,7 @@ void bh_params_default(bh_params *p) {
   p->strict_keys = 1;
 }
 
-const char *bh_version(void) { return "hierarquicos-b200 0.1.0 (sm_100a)"; }
+const char *bh_version(void) { return "hierarquicos-b200 0.2.0 (sm_100a)"; }
 
 int bh_last_error(char *buf, int len) {
   if (buf && len > 0) {
@@ -283,38 +486,24 @@ int bh_system_destroy(bh_system *s) {
   if (!s) return BH_OK;
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
-  free_buffers(s->b);
+  drop_graph(s);
+  if (!s->fixed_buffers) free_buffers(s->b);
   delete s;
   return BH_OK;
 }
 
 int bh_system_build(bh_system *s, const double *d_m, const double *d_x, const double *d_y,
                     const double *d_z, int64_t n, const bh_params *p, void *stream) {
-  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
-  int rc = check_params(p, n);
-  if (rc) return rc;
-  if (!d_m || !d_x || !d_y || !d_z) return set_err(BH_ERR_INVALID, "NULL input array");
-  BH_CUDA(cudaSetDevice(s->device));
-  s->p = *p;
-  rc = ensure_capacity(s, n);
-  if (rc) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  s->m = d_m; s->x = d_x; s->y = d_y; s->z = d_z;
-  s->n = n;
-  s->order = p->order;
-  s->walked = 0;
-  if (n == 1) {
-    // a lone body feels no force; there is no extent to normalise by
-    BH_CUDA(cudaMemsetAsync(s->b.sc, 0, sizeof(bh::Scalars), st));
-    s->built = 1;
-    s->keys_checked = 1;
-    return BH_OK;
-  }
-  enqueue_build(s, n, 0, st);
-  BH_CUDA(cudaGetLastError());
-  s->built = 1;
-  s->keys_checked = p->strict_keys ? 0 : 1;
-  return BH_OK;
+  if (n < 1 || n > (int64_t)(1 << 30))
+    return set_err(BH_ERR_INVALID, "n=%lld out of range [1, 2^30]", (long long)n);
+  const int64_t off[2] = {0, n};
+  return build_common(s, d_m, d_x, d_y, d_z, off, 1, p, (cudaStream_t)stream);
+}
+
+int bh_system_build_batch(bh_system *s, const double *d_m, const double *d_x,
+                          const double *d_y, const double *d_z, const int64_t *offsets,
+                          int nsys, const bh_params *p, void *stream) {
+  return build_common(s, d_m, d_x, d_y, d_z, offsets, nsys, p, (cudaStream_t)stream);
 }
 
 int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream) {
@@ -325,72 +514,18 @@ int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream
   if (p->order > s->order) return set_err(BH_ERR_INVALID, "order %d above the built order %d", p->order, s->order);
   if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
   BH_CUDA(cudaSetDevice(s->device));
-  cudaStream_t st = (cudaStream_t)stream;
-  const int64_t n = s->n;
-  if (n == 1) {
-    BH_CUDA(cudaMemsetAsync(d_out, 0, 3 * sizeof(double), st));
-  } else {
-    bh::WalkParams w = walk_params(p, s->order);
-    if (w.count_stats) BH_CUDA(cudaMemsetAsync(s->b.stats, 0, 4 * sizeof(unsigned long long), st));
-    if (p->precision == BH_PREC_REFERENCE)
-      bh::launch_reference_walk(n, w, s->b, d_out, nullptr, 0, nullptr, st);
-    else
-      bh::launch_walk(n, w, s->b, d_out, st);
-  }
+  enqueue_walk(s, p, d_out, (cudaStream_t)stream);
+  BH_CUDA(cudaGetLastError());
   s->walked = 1;
   s->walk_p = *p;
   s->walk_out = d_out;
-  BH_CUDA(cudaGetLastError());
   return BH_OK;
 }
 
-namespace {
-
-// Completes a build + walk: strict-key check (slow path only when a body lies
-// within the rounding margin of a cell edge), stack-capacity retries, status.
-int finish(bh_system *s, cudaStream_t st) {
-  int rc = read_scalars(s, st);
-  if (rc) return rc;
-  if (!s->keys_checked && (s->b.sc_host->key_ambiguous || s->p.strict_keys == 2) &&
-      !(s->b.sc_host->err & bh::kErrNonFinite)) {
-    // the reference's sequential centre of mass decides the ambiguous keys
-    bh::launch_seq_com(s->m, s->x, s->y, s->z, s->n, s->p.com_mode, s->b, st);
-    bh::launch_verify_keys(s->m, s->x, s->y, s->z, s->n, s->p.depth, s->b, st);
-    rc = read_scalars(s, st);
-    if (rc) return rc;
-    if (s->b.sc_host->key_mismatch) {
-      bh::launch_adopt_seq_com(s->b, st);
-      enqueue_build(s, s->n, 1, st);
-      if (s->walked) {
-        rc = bh_system_walk(s, &s->walk_p, s->walk_out, st);
-        if (rc) return rc;
-      }
-      rc = read_scalars(s, st);
-      if (rc) return rc;
-    }
-  }
-  s->keys_checked = 1;
-  for (int attempt = 0;
-       attempt < 4 && s->walked && !s->fixed_buffers && (s->b.sc_host->err & bh::kErrStackOverflow);
-       ++attempt) {
-    s->stack_cap *= 2;
-    rc = ensure_capacity(s, s->n);
-    if (rc) return rc;
-    BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
-    rc = bh_system_walk(s, &s->walk_p, s->walk_out, st);
-    if (rc) return rc;
-    rc = read_scalars(s, st);
-    if (rc) return rc;
-  }
-  return status_from_device(s, 0);
-}
-
-}  // namespace
-
 int bh_system_sync(bh_system *s, void *stream) {
   if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
-  BH_CUDA(cudaSetDevice(s->device));
   if (!s->built) return set_err(BH_ERR_NOT_BUILT, "sync before build");
+  BH_CUDA(cudaSetDevice(s->device));
   return finish(s, (cudaStream_t)stream);
 }
 
@@ -404,6 +539,65 @@ int bh_system_forces(bh_system *s, const double *d_m, const double *d_x, const d
   return finish(s, (cudaStream_t)stream);
 }
 
+int bh_system_forces_batch(bh_system *s, const double *d_m, const double *d_x,
+                           const double *d_y, const double *d_z, const int64_t *offsets,
+                           int nsys, const bh_params *p, double *d_out, void *stream) {
+  int rc = bh_system_build_batch(s, d_m, d_x, d_y, d_z, offsets, nsys, p, stream);
+  if (rc) return rc;
+  rc = bh_system_walk(s, p, d_out, stream);
+  if (rc) return rc;
+  return finish(s, (cudaStream_t)stream);
+}
+
+int bh_system_capture(bh_system *s, const bh_params *p, double *d_out) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (!s->built) return set_err(BH_ERR_NOT_BUILT, "capture needs a build of the batch first");
+  int rc = check_params(p, s->n);
+  if (rc) return rc;
+  if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
+  BH_CUDA(cudaSetDevice(s->device));
+  BH_CUDA(cudaDeviceSynchronize());
+  drop_graph(s);
+  cudaStream_t cap = nullptr;
+  BH_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  const bh_params saved = s->p;
+  const int saved_order = s->order;
+  s->p = *p;
+  s->order = p->order;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue_build(s, 0, cap);
+    enqueue_walk(s, p, d_out, cap);
+    e = cudaStreamEndCapture(cap, &g);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  if (e != cudaSuccess) {
+    s->graph = nullptr;
+    s->p = saved;
+    s->order = saved_order;
+    cudaGetLastError();
+    return set_err(BH_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  }
+  s->walk_p = *p;
+  s->walk_out = d_out;
+  s->built = 0;  // nothing ran yet: the first replay builds
+  return BH_OK;
+}
+
+int bh_system_replay(bh_system *s, void *stream) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (!s->graph) return set_err(BH_ERR_NOT_BUILT, "replay before capture");
+  BH_CUDA(cudaSetDevice(s->device));
+  BH_CUDA(cudaGraphLaunch(s->graph, (cudaStream_t)stream));
+  s->built = 1;
+  s->walked = 1;
+  s->keys_checked = s->p.strict_keys ? 0 : 1;
+  return BH_OK;
+}
+
 int bh_system_info(bh_system *s, int64_t *n, int *depth, int64_t *n_nodes, int64_t *n_groups,
                    double *com4, double *ssa) {
   if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
@@ -412,12 +606,31 @@ int bh_system_info(bh_system *s, int64_t *n, int *depth, int64_t *n_nodes, int64
   int rc = read_scalars(s, 0);
   if (rc) return rc;
   const bh::Scalars &h = *s->b.sc_host;
+  bh::SysScalars s0;
+  BH_CUDA(cudaMemcpy(&s0, s->b.ss, sizeof s0, cudaMemcpyDeviceToHost));
   if (n) *n = s->n;
   if (depth) *depth = h.L;
-  if (n_nodes) *n_nodes = s->n >= 2 ? h.n_compact : 0;
-  if (n_groups) *n_groups = s->n >= 2 ? h.n_groups : 0;
-  if (com4) { com4[0] = h.com[0]; com4[1] = h.com[1]; com4[2] = h.com[2]; com4[3] = h.mass; }
-  if (ssa) *ssa = h.ssa;
+  if (n_nodes) *n_nodes = h.n_compact;
+  if (n_groups) *n_groups = h.n_groups;
+  if (com4) { com4[0] = s0.com[0]; com4[1] = s0.com[1]; com4[2] = s0.com[2]; com4[3] = s0.mass; }
+  if (ssa) *ssa = s0.ssa;
+  return BH_OK;
+}
+
+int bh_system_batch_info(bh_system *s, int32_t *roots, double *com4, double *ssa) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (!s->built) return set_err(BH_ERR_NOT_BUILT, "info before build");
+  BH_CUDA(cudaSetDevice(s->device));
+  BH_CUDA(cudaDeviceSynchronize());
+  std::vector<bh::SysScalars> h((size_t)s->nsys);
+  BH_CUDA(cudaMemcpy(h.data(), s->b.ss, h.size() * sizeof(bh::SysScalars), cudaMemcpyDeviceToHost));
+  for (int q = 0; q < s->nsys; ++q) {
+    if (roots) roots[q] = h[q].root;
+    if (com4)
+      for (int k = 0; k < 3; ++k) com4[4 * q + k] = h[q].com[k];
+    if (com4) com4[4 * q + 3] = h[q].mass;
+    if (ssa) ssa[q] = h[q].ssa;
+  }
   return BH_OK;
 }
 
@@ -436,7 +649,7 @@ int bh_system_get_nodes(bh_system *s, int32_t *meta4, int32_t *child8, int32_t *
   BH_CUDA(cudaSetDevice(s->device));
   int rc = read_scalars(s, 0);
   if (rc) return rc;
-  const int64_t M = s->n >= 2 ? s->b.sc_host->n_compact : 0;
+  const int64_t M = s->b.sc_host->n_compact;
   const Buffers &b = s->b;
   if (M > 0) {
     if (meta4) BH_CUDA(cudaMemcpy(meta4, b.cn_meta, M * sizeof(int4), cudaMemcpyDeviceToHost));
@@ -446,7 +659,7 @@ int bh_system_get_nodes(bh_system *s, int32_t *meta4, int32_t *child8, int32_t *
     if (quad6 && s->order >= 4) BH_CUDA(cudaMemcpy(quad6, b.cn_quad, M * 6 * sizeof(double), cudaMemcpyDeviceToHost));
     if (oct14 && s->order >= 8) BH_CUDA(cudaMemcpy(oct14, b.cn_oct, M * 14 * sizeof(double), cudaMemcpyDeviceToHost));
   }
-  if (level_begin && s->n >= 2)
+  if (level_begin)
     BH_CUDA(cudaMemcpy(level_begin, b.level_begin, (s->b.sc_host->L + 2) * sizeof(int32_t), cudaMemcpyDeviceToHost));
   return BH_OK;
 }
@@ -456,7 +669,7 @@ int bh_system_get_groups(bh_system *s, int32_t *group_first) {
   BH_CUDA(cudaSetDevice(s->device));
   int rc = read_scalars(s, 0);
   if (rc) return rc;
-  if (s->n >= 2 && group_first)
+  if (group_first)
     BH_CUDA(cudaMemcpy(group_first, s->b.g_first, (s->b.sc_host->n_groups + 1) * sizeof(int32_t),
                        cudaMemcpyDeviceToHost));
   return BH_OK;
@@ -479,13 +692,9 @@ int bh_system_reference_targets(bh_system *s, const bh_params *p, const int64_t 
   if (!d_targets || ntargets < 1 || !d_out) return set_err(BH_ERR_INVALID, "bad targets/output");
   if (p->order > s->order) return set_err(BH_ERR_INVALID, "order above the built order");
   BH_CUDA(cudaSetDevice(s->device));
-  cudaStream_t st = (cudaStream_t)stream;
-  if (s->n == 1) {
-    BH_CUDA(cudaMemsetAsync(d_out, 0, 3 * ntargets * sizeof(double), st));
-    return BH_OK;
-  }
   bh::WalkParams w = walk_params(p, s->order);
-  bh::launch_reference_walk(s->n, w, s->b, d_out, d_targets, ntargets, d_counts, st);
+  bh::launch_reference_walk(s->n, w, s->b, d_out, d_targets, ntargets, d_counts,
+                            (cudaStream_t)stream);
   BH_CUDA(cudaGetLastError());
   return BH_OK;
 }
@@ -499,16 +708,10 @@ int bh_compute_forces_ex(const double *m, const double *x, const double *y, cons
   bh_system *s = nullptr;
   rc = default_system(&s);
   if (rc) return rc;
-  rc = ensure_capacity(s, n);
-  if (rc) return rc;
-  rc = ensure_host_staging(s, n);
-  if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  rc = stage_inputs(s, m, x, y, z, n, st);
+  if (rc) return rc;
   Buffers &b = s->b;
-  BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
   rc = bh_system_forces(s, b.hm, b.hx, b.hy, b.hz, n, p, b.hout, stream);
   if (rc) return rc;
   BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -539,16 +742,10 @@ int bh_compute_forces_direct(const double *m, const double *x, const double *y,
   bh_system *s = nullptr;
   int rc = default_system(&s);
   if (rc) return rc;
-  rc = ensure_capacity(s, n);
-  if (rc) return rc;
-  rc = ensure_host_staging(s, n);
-  if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  rc = stage_inputs(s, m, x, y, z, n, st);
+  if (rc) return rc;
   Buffers &b = s->b;
-  BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
   bh::launch_direct(b.hm, b.hx, b.hy, b.hz, n, nullptr, 0, G, eps * eps, out_kind, b.hout, st);
   BH_CUDA(cudaGetLastError());
   BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));

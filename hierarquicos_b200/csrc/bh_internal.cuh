@@ -25,29 +25,58 @@ enum DeviceError : int {
   kErrChildren = 1 << 4,       // more than 8 children (a bug)
 };
 
-// Scalars computed on the device for one system.  Plain doubles so that the
-// host can read them back with a single copy.
-struct Scalars {
-  double bmin[3], bmax[3];  // bounding box of the positions
-  double com[3], mass;      // centre of mass used for the keys
-  double com_seq[3], mass_seq;  // centre of mass in the reference's order
-  double ssa;               // side of the root cube, amp * largest extent
-  double vcen[3];           // centre of the normalised box (keys)
-  double vcen_seq[3];
-  int L;                    // key depth actually used
-  int n_compact;            // number of compact internal nodes
-  int n_groups;             // number of target groups
-  int err;                  // DeviceError bits
-  int key_mismatch;         // keys differ from the sequential-COM keys
-  int max_lcp;              // deepest shared octal prefix (auto depth)
-  int key_ambiguous;        // some body lies within the rounding margin of a cell edge
-  int pad;
-  double key_margin;        // that margin, in units of the finest cell
+// A batch is a set of independent systems stored back to back: system s owns
+// bodies [off, off + n) of the concatenated arrays, in the caller's order, and
+// after the sort the same range in key order.  Every kernel runs once for the
+// whole batch; a lone system is a batch of one.
+
+// Scalars of one system, computed on the device.  Plain doubles so that the
+// host can read them back with one copy.
+struct SysScalars {
+  double bmin[3], bmax[3];      // bounding box of the positions
+  double com[3], mass;          // centre of mass used for the keys
+  double com_seq[3], mass_seq;  // centre of mass in the reference's sequential order
+  double ssa;                   // side of the root cube, amp * largest extent
+  double vcen[3];               // centre of the normalised box (keys)
+  double key_margin;            // rounding margin of the keys, in finest cells
+  int64_t off, n;               // the system's range of bodies
+  int root;                     // compact node of the system's root, -1 if n < 2
+  int key_ambiguous;            // a body lies within the rounding margin of a cell edge
+  int key_mismatch;             // a key differs from the sequential-sum key
+  int err;                      // DeviceError bits of this system
 };
 
-// Per-system device buffers.  Sized for `cap` particles.
+// Batch-wide scalars.
+struct Scalars {
+  int L;              // key depth actually used
+  int n_compact;      // compact internal nodes of all systems
+  int n_groups;       // target groups of all systems
+  int err;            // DeviceError bits of any system
+  int key_mismatch;   // any system
+  int key_ambiguous;  // any system
+  int max_lcp;        // deepest shared octal prefix (automatic depth, one system)
+  int nsys;
+};
+
+// Work item of the per-system reductions: bodies [start, end) of system sys.
+struct RedItem {
+  int sys, pad;
+  int64_t start, end;
+};
+constexpr int64_t kRedChunk = 8192;
+
+// Device workspace of a batch.  Sized for `cap` bodies and `sys_cap` systems.
 struct Buffers {
   int64_t cap = 0;
+  int sys_cap = 0;
+  // batch layout
+  int nsys = 0;
+  SysScalars *ss = nullptr;        // nsys entries
+  SysScalars *ss_host = nullptr;   // host mirror
+  int32_t *sys_of = nullptr;       // system of each body (same in input and key order)
+  RedItem *items = nullptr;        // reduction work items
+  int n_items = 0;
+  int items_cap = 0;
   // inputs staged from the host (host-pointer API only)
   double *hm = nullptr, *hx = nullptr, *hy = nullptr, *hz = nullptr;
   double *hout = nullptr;
@@ -76,7 +105,6 @@ struct Buffers {
   int32_t *level_begin = nullptr;  // kNumLevels + 1 entries
   // target groups
   int32_t *gflag = nullptr, *gscan = nullptr, *g_first = nullptr;
-  int32_t *inv_perm = nullptr;
   // scan scratch
   int32_t *scan_tmp = nullptr;
   int64_t scan_tmp_cap = 0;
@@ -92,13 +120,16 @@ struct Buffers {
 
 // ---- kernels / launchers (one translation unit each) ----
 
-// keys: bbox + COM + keys.  com_mode: 0 separate multiply and add, 1 fused.
+// batch layout: sys_of from the per-system offsets in `ss`
+void launch_layout(Buffers &b, cudaStream_t s);
+// keys: bbox + COM + keys of every system.  com_mode: 0 separate multiply and
+// add, 1 fused.
 void launch_keys(const double *m, const double *x, const double *y, const double *z, int64_t n,
                  int L, double amp, int com_mode, Buffers &b, cudaStream_t s);
 void launch_seq_com(const double *m, const double *x, const double *y, const double *z,
-                    int64_t n, int com_mode, Buffers &b, cudaStream_t s);
-void launch_verify_keys(const double *m, const double *x, const double *y, const double *z,
-                        int64_t n, int L, Buffers &b, cudaStream_t s);
+                    int com_mode, int all, Buffers &b, cudaStream_t s);
+void launch_verify_keys(const double *x, const double *y, const double *z, int64_t n, int all,
+                        Buffers &b, cudaStream_t s);
 void launch_auto_depth(int64_t n, Buffers &b, cudaStream_t s);
 void launch_adopt_seq_com(Buffers &b, cudaStream_t s);
 void launch_keys_only(const double *x, const double *y, const double *z, int64_t n, int L,
@@ -129,9 +160,12 @@ void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s);
+// after the key sort of a batch: stable sort by system, so that every system's
+// bodies are again contiguous, in key order
+void launch_sort_by_system(int64_t n, Buffers &b, cudaStream_t s);
 void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s);
 void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s);
-void launch_groups(int64_t n, int group_size, Buffers &b, cudaStream_t s);
+void launch_groups(int64_t n, int group_size, int group_span, Buffers &b, cudaStream_t s);
 
 struct WalkParams {
   double theta2, G, eps2;
@@ -161,5 +195,6 @@ struct bh_system;
 int bh_report_error(int code, const char *msg);
 namespace bh {
 // bh_abi.cu: a system whose workspace is `b` (caller-owned, never grown)
-bh_system *fixed_system_create(int device, const Buffers &b, Scalars *host_sc);
+bh_system *fixed_system_create(int device, const Buffers &b, Scalars *host_sc,
+                               SysScalars *host_ss);
 }  // namespace bh

@@ -16,7 +16,8 @@
 //    module holding it is loaded, until the process exits;
 //  * the first call on a device looks the array's device address up
 //    (cudaGetSymbolAddress, with that device current) and keeps it; later
-//    calls on that device reuse it;
+//    calls on that device reuse it.  Make that first call before any stream
+//    capture begins, so that the set-up does not happen inside one;
 //  * all calls on a device share the one array, which keeps the last call's
 //    contents; every call initialises what it reads.  Calls that overlap on
 //    the GPU (other streams, other host threads) race on that array: issue
@@ -37,7 +38,8 @@ namespace {
 constexpr int64_t kMaxN = BH_NOALLOC_MAX_N;
 constexpr int64_t kSlots = 512;       // warp slots of the walk (128 blocks of 4 warps)
 constexpr int64_t kStackCap = 1024;   // stack entries per warp slot
-constexpr int kNumBufs = 33;
+constexpr int64_t kItems = (kMaxN + bh::kRedChunk - 1) / bh::kRedChunk;  // reduction items
+constexpr int kNumBufs = 36;
 
 constexpr int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
 
@@ -53,7 +55,10 @@ constexpr Sizes buffer_bytes(int64_t c) {
   z.v[i++] = 4 * c;                                   // v0
   z.v[i++] = 4 * c;                                   // v1
   z.v[i++] = 4 * bh::radix_hist_entries(c);           // hist
-  z.v[i++] = 8 * 296 * 10;                            // partials
+  z.v[i++] = 8 * 10 * kItems;                         // partials
+  z.v[i++] = (int64_t)sizeof(bh::SysScalars);          // ss (one system)
+  z.v[i++] = 4 * c;                                   // sys_of
+  z.v[i++] = (int64_t)sizeof(bh::RedItem) * kItems;    // items
   z.v[i++] = 32 * c;                                  // spos
   for (int k = 0; k < 8; ++k) z.v[i++] = 4 * c;       // bn_* and bin2cn
   z.v[i++] = 4 * c;                                   // cn_bin
@@ -98,7 +103,8 @@ bh::Buffers carve(unsigned char *base) {
     off += align256(z.v[i++]);
   };
   bh::Buffers b;
-  take(b.k0); take(b.k1); take(b.v0); take(b.v1); take(b.hist); take(b.partials); take(b.spos);
+  take(b.k0); take(b.k1); take(b.v0); take(b.v1); take(b.hist); take(b.partials); take(b.ss);
+  take(b.sys_of); take(b.items); take(b.spos);
   take(b.bn_left); take(b.bn_right); take(b.bn_parent); take(b.bn_first); take(b.bn_last);
   take(b.bn_level); take(b.bn_flag); take(b.bin2cn);
   take(b.cn_bin); take(b.cn_meta); take(b.cn_child); take(b.cn_parent); take(b.cn_com);
@@ -106,6 +112,8 @@ bh::Buffers carve(unsigned char *base) {
   take(b.gflag); take(b.gscan); take(b.g_first); take(b.scan_tmp); take(b.wstack);
   take(b.counters); take(b.stats); take(b.sc);
   b.cap = kMaxN;
+  b.sys_cap = 1;
+  b.items_cap = (int)kItems;
   b.hist_cap = bh::radix_hist_entries(kMaxN);
   b.scan_tmp_cap = bh::scan_tmp_entries(kMaxN + 1);
   b.wstack_cap = kStackCap;
@@ -116,6 +124,7 @@ bh::Buffers carve(unsigned char *base) {
 struct DeviceWorkspace {
   bh_system *sys = nullptr;
   bh::Scalars host_sc{};
+  bh::SysScalars host_ss{};
 };
 
 std::mutex g_mu;
@@ -151,7 +160,8 @@ extern "C" int bh_compute_forces_noalloc(const double *d_m, const double *d_x, c
                cudaGetErrorString(e));
       return bh_report_error(BH_ERR_CUDA, g_msg);
     }
-    w.sys = bh::fixed_system_create(dev, carve(static_cast<unsigned char *>(base)), &w.host_sc);
+    w.sys = bh::fixed_system_create(dev, carve(static_cast<unsigned char *>(base)), &w.host_sc,
+                                      &w.host_ss);
   }
   return bh_system_forces(w.sys, d_m, d_x, d_y, d_z, n, p, d_out, stream);
 }

@@ -241,6 +241,29 @@ gather_kernel(const double *__restrict__ m, const double *__restrict__ x,
   }
 }
 
+// stage 2 of a batch sort: key = system of the body at sorted position i
+__global__ void __launch_bounds__(256)
+sys_keys_kernel(const int32_t *__restrict__ perm, const int32_t *__restrict__ sys_of, int64_t n,
+                uint64_t *__restrict__ ck, int32_t *__restrict__ cv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    ck[i] = (uint64_t)sys_of[perm[i]];
+    cv[i] = (int32_t)i;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+regather_kernel(const uint64_t *__restrict__ k0, const int32_t *__restrict__ v0,
+                const int32_t *__restrict__ order, int64_t n, uint64_t *__restrict__ k1,
+                int32_t *__restrict__ v1) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t j = order[i];
+    k1[i] = k0[j];
+    v1[i] = v0[j];
+  }
+}
+
 bool g_sort_attr_set = false;
 
 }  // namespace
@@ -288,6 +311,25 @@ void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int6
 }
 
 
+
+// The key sort orders all bodies of a batch by key; a stable sort by system
+// then restores the systems' ranges with each range in key order (LSD order:
+// the system is the most significant part of the (system, key) pair).
+void launch_sort_by_system(int64_t n, Buffers &b, cudaStream_t s) {
+  if (b.nsys < 2) return;
+  int bits = 1;
+  while ((1 << bits) < b.nsys) ++bits;
+  uint64_t *ck0 = reinterpret_cast<uint64_t *>(b.cn_quad);       // scratch until the upward pass
+  uint64_t *ck1 = reinterpret_cast<uint64_t *>(b.cn_quad) + b.cap;
+  int32_t *cv0 = b.cn_parent;                                    // scratch until the records
+  int32_t *cv1 = b.bn_flag;                                      // scratch until the marks
+  const int grid = grid_for(n, 256, 148 * 16);
+  sys_keys_kernel<<<grid, 256, 0, s>>>(b.v0, b.sys_of, n, ck0, cv0);
+  radix_sort_pairs(ck0, cv0, ck1, cv1, n, nullptr, bits, b.hist, s);
+  regather_kernel<<<grid, 256, 0, s>>>(b.k0, b.v0, cv0, n, b.k1, b.v1);
+  cudaMemcpyAsync(b.k0, b.k1, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(b.v0, b.v1, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+}
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s) {

@@ -20,43 +20,52 @@
 // parent's starts a new octree node.  Those nodes are sorted by (level, first
 // particle) with the radix sort, and each one enumerates its octree children
 // by descending at most three binary levels.
+//
+// In a batch every system is its own segment of the sorted arrays: the
+// binary tree of a segment [s0, s1) uses internal nodes s0 .. s1 - 2 (the slot
+// s1 - 1 stays unused) and treats bodies outside the segment as absent, so
+// every system gets its own root; all later steps run over all systems at once.
 #include "bh_internal.cuh"
 
 namespace bh {
 
 namespace {
 
-__device__ __forceinline__ int delta(const uint64_t *__restrict__ k, int64_t n, int64_t i,
-                                     uint64_t ki, int64_t j) {
-  if (j < 0 || j >= n) return -1;
+__device__ __forceinline__ int delta(const uint64_t *__restrict__ k, int64_t s0, int64_t s1,
+                                     int64_t i, uint64_t ki, int64_t j) {
+  if (j < s0 || j >= s1) return -1;
   uint64_t kj = k[j];
   if (ki != kj) return __clzll((long long)(ki ^ kj));
   return 64 + __clz((int)(i ^ j));
 }
 
 __global__ void __launch_bounds__(256)
-karras_kernel(const uint64_t *__restrict__ k, int64_t n, const Scalars *__restrict__ sc,
+karras_kernel(const uint64_t *__restrict__ k, int64_t n, const int32_t *__restrict__ sys_of,
+              const SysScalars *__restrict__ sys, const Scalars *__restrict__ sc,
               int32_t *__restrict__ left, int32_t *__restrict__ right,
               int32_t *__restrict__ parent, int32_t *__restrict__ first,
               int32_t *__restrict__ last, int32_t *__restrict__ level) {
   const int L = sc->L;
   const int lead = 64 - 3 * L;  // leading zero bits of every key
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
+    const SysScalars &ss = sys[sys_of[i]];
+    const int64_t s0 = ss.off, s1 = ss.off + ss.n;
+    if (i == s1 - 1) continue;  // the segment's unused slot (marked by mark_kernel)
     const uint64_t ki = k[i];
-    const int d = (delta(k, n, i, ki, i + 1) - delta(k, n, i, ki, i - 1)) > 0 ? 1 : -1;
-    const int dmin = delta(k, n, i, ki, i - d);
+    const int d = (delta(k, s0, s1, i, ki, i + 1) - delta(k, s0, s1, i, ki, i - 1)) > 0 ? 1 : -1;
+    const int dmin = delta(k, s0, s1, i, ki, i - d);
     int64_t lmax = 2;
-    while (delta(k, n, i, ki, i + lmax * d) > dmin) lmax <<= 1;
+    while (delta(k, s0, s1, i, ki, i + lmax * d) > dmin) lmax <<= 1;
     int64_t l = 0;
     for (int64_t t = lmax >> 1; t >= 1; t >>= 1)
-      if (delta(k, n, i, ki, i + (l + t) * d) > dmin) l += t;
+      if (delta(k, s0, s1, i, ki, i + (l + t) * d) > dmin) l += t;
     const int64_t j = i + l * d;
-    const int dnode = delta(k, n, i, ki, j);
+    const int dnode = delta(k, s0, s1, i, ki, j);
     int64_t s = 0, t = l;
     do {
       t = (t + 1) >> 1;
-      if (delta(k, n, i, ki, i + (s + t) * d) > dnode) s += t;
+      if (delta(k, s0, s1, i, ki, i + (s + t) * d) > dnode) s += t;
     } while (t > 1);
     const int64_t gamma = i + s * d + (d < 0 ? -1 : 0);
     const int64_t f = min(i, j), la = max(i, j);
@@ -70,17 +79,20 @@ karras_kernel(const uint64_t *__restrict__ k, int64_t n, const Scalars *__restri
     level[i] = v > L ? L : v;
     if (lc >= 0) parent[lc] = (int32_t)i;
     if (rc >= 0) parent[rc] = (int32_t)i;
-    if (i == 0) parent[0] = -1;
+    if (i == s0) parent[i] = -1;  // the segment's root
   }
 }
 
 __global__ void __launch_bounds__(256)
-mark_kernel(int64_t n, const int32_t *__restrict__ parent, const int32_t *__restrict__ level,
+mark_kernel(int64_t n, const int32_t *__restrict__ sys_of, const SysScalars *__restrict__ sys,
+            const int32_t *__restrict__ parent, const int32_t *__restrict__ level,
             int32_t *__restrict__ flag) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    int p = parent[i];
-    flag[i] = (i == 0 || level[i] > level[p]) ? 1 : 0;
+    const SysScalars &ss = sys[sys_of[i]];
+    if (i == ss.off + ss.n - 1) { flag[i] = 0; continue; }  // unused slot
+    const int p = parent[i];
+    flag[i] = (p < 0 || level[i] > level[p]) ? 1 : 0;
   }
 }
 
@@ -88,7 +100,7 @@ __global__ void __launch_bounds__(256)
 compact_keys_kernel(int64_t n, const int32_t *__restrict__ flag, const int32_t *__restrict__ rank,
                     const int32_t *__restrict__ level, const int32_t *__restrict__ first,
                     int first_bits, uint64_t *__restrict__ ckey, int32_t *__restrict__ cval) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     if (!flag[i]) continue;
     int r = rank[i];
@@ -146,8 +158,7 @@ records_kernel(const int32_t *__restrict__ order, Scalars *__restrict__ sc,
     meta[j] = make_int4(f, la - f + 1, v, nc);
     for (int c = 0; c < 8; ++c) child[8 * j + c] = c < nc ? ch[c] : 0x7fffffff;
     for (int c = 0; c < nc; ++c)
-      if (ch[c] >= 0) cparent[ch[c]] = j;
-    if (j == 0) cparent[0] = -1;
+      if (ch[c] >= 0) cparent[ch[c]] = j;  // roots keep the -1 of the initial fill
   }
   if (err) atomicOr(&sc->err, err);
 }
@@ -164,6 +175,14 @@ level_begin_kernel(const int4 *__restrict__ meta, const Scalars *__restrict__ sc
   }
 }
 
+// root node of every system (its segment's binary root), -1 for lone bodies
+__global__ void roots_kernel(SysScalars *__restrict__ sys, int nsys,
+                             const int32_t *__restrict__ bin2cn) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  sys[s].root = sys[s].n >= 2 ? bin2cn[sys[s].off] : -1;
+}
+
 __global__ void count_to_scalars(const int32_t *__restrict__ total, Scalars *sc, int which) {
   if (threadIdx.x == 0) {
     if (which == 0) sc->n_compact = *total;
@@ -172,35 +191,56 @@ __global__ void count_to_scalars(const int32_t *__restrict__ total, Scalars *sc,
 }
 
 // ---- target groups ----
-// Each node with more than G bodies packs its consecutive small children
-// (lone particles and nodes with <= G bodies) greedily into groups of <= G
-// bodies; a big child closes the open group.  A node of identical keys (no
-// children) is cut into chunks of G.  gflag marks the first body of each group.
+// Units are the subtrees of <= U bodies whose parent holds more than U bodies
+// (lone particles included).  Consecutive units under the same parent are
+// concatenated in key order and cut into groups of G bodies (the last one of a
+// run shorter); a child with more than U bodies ends the run and is cut by its
+// own children.  A node of identical keys (no children) with more than U
+// bodies, or a root of <= U bodies, is cut into groups of G directly.
+// gflag marks the first body of each group.  With U = G this packs small
+// siblings; a larger U fills more groups completely at the price of groups
+// that span neighbouring subtrees.
 __global__ void __launch_bounds__(256)
 group_flags_kernel(const int4 *__restrict__ meta, const int32_t *__restrict__ child,
-                   const Scalars *__restrict__ sc, int G, int32_t *__restrict__ gflag) {
+                   const int32_t *__restrict__ cparent, const Scalars *__restrict__ sc, int G,
+                   int U, int32_t *__restrict__ gflag) {
   const int M = sc->n_compact;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
     const int4 mt = meta[j];  // first, count, level, nchild
-    if (mt.y <= G) {
-      if (j == 0) gflag[mt.x] = 1;
+    if (mt.y <= U) {
+      if (cparent[j] < 0)  // a system's root
+        for (int s = 0; s < mt.y; s += G) gflag[mt.x + s] = 1;
       continue;
     }
     if (mt.w == 0) {
       for (int s = 0; s < mt.y; s += G) gflag[mt.x + s] = 1;
       continue;
     }
-    int cur = 0;
-    for (int c = 0; c < mt.w; ++c) {
-      int32_t ch = child[8 * j + c];
-      int cfirst, ccount;
-      if (ch < 0) { cfirst = ~ch; ccount = 1; }
-      else { int4 cm = meta[ch]; cfirst = cm.x; ccount = cm.y; }
-      if (ccount > G) { cur = 0; continue; }
-      if (cur == 0 || cur + ccount > G) { gflag[cfirst] = 1; cur = ccount; }
-      else cur += ccount;
+    int run_first = -1, run_len = 0;
+    for (int c = 0; c <= mt.w; ++c) {
+      int cfirst = 0, ccount = U + 1;  // c == nchild: closes the last run
+      if (c < mt.w) {
+        const int32_t ch = child[8 * j + c];
+        if (ch < 0) { cfirst = ~ch; ccount = 1; }
+        else { const int4 cm = meta[ch]; cfirst = cm.x; ccount = cm.y; }
+      }
+      if (ccount > U) {
+        for (int s = 0; s < run_len; s += G) gflag[run_first + s] = 1;
+        run_first = -1;
+        run_len = 0;
+        continue;
+      }
+      if (run_first < 0) run_first = cfirst;
+      run_len += ccount;
     }
   }
+}
+
+// every system starts a group (this also covers lone bodies, which have no node)
+__global__ void system_starts_kernel(const SysScalars *__restrict__ sys, int nsys,
+                                     int32_t *__restrict__ gflag) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsys && sys[s].n > 0) gflag[sys[s].off] = 1;
 }
 
 __global__ void __launch_bounds__(256)
@@ -223,13 +263,13 @@ int bits_for(int64_t v) {
 void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s) {
   (void)L;
   const int grid = grid_for(n, 256, 148 * 16);
-  karras_kernel<<<grid, 256, 0, s>>>(b.k0, n, b.sc, b.bn_left, b.bn_right, b.bn_parent,
-                                     b.bn_first, b.bn_last, b.bn_level);
-  mark_kernel<<<grid, 256, 0, s>>>(n, b.bn_parent, b.bn_level, b.bn_flag);
+  karras_kernel<<<grid, 256, 0, s>>>(b.k0, n, b.sys_of, b.ss, b.sc, b.bn_left, b.bn_right,
+                                     b.bn_parent, b.bn_first, b.bn_last, b.bn_level);
+  mark_kernel<<<grid, 256, 0, s>>>(n, b.sys_of, b.ss, b.bn_parent, b.bn_level, b.bn_flag);
   // rank of each marked node in binary order, total -> n_compact
   int32_t *rank = b.gscan;          // free until the group pass
   int32_t *total = b.counters + 2;  // scratch counter
-  exclusive_scan(b.bn_flag, rank, n - 1, nullptr, total, b.scan_tmp, s);
+  exclusive_scan(b.bn_flag, rank, n, nullptr, total, b.scan_tmp, s);
   count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 0);
   // sort the compact nodes by (level, first particle)
   const int first_bits = bits_for(n);
@@ -239,19 +279,23 @@ void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s) {
   int32_t *cv1 = b.cn_parent;                                // scratch: filled later
   compact_keys_kernel<<<grid, 256, 0, s>>>(n, b.bn_flag, rank, b.bn_level, b.bn_first, first_bits,
                                            ck0, cv0);
-  radix_sort_pairs(ck0, cv0, ck1, cv1, n - 1, total, first_bits + 5, b.hist, s);
-  cudaMemcpyAsync(b.cn_bin, cv0, (n - 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+  radix_sort_pairs(ck0, cv0, ck1, cv1, n, total, first_bits + 5, b.hist, s);
+  cudaMemcpyAsync(b.cn_bin, cv0, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+  cudaMemsetAsync(b.cn_parent, 0xff, n * sizeof(int32_t), s);  // roots keep -1
   bin2cn_kernel<<<grid, 256, 0, s>>>(b.cn_bin, b.sc, b.bin2cn);
   records_kernel<<<grid, 256, 0, s>>>(b.cn_bin, b.sc, b.bn_left, b.bn_right, b.bn_first,
                                       b.bn_last, b.bn_level, b.bn_flag, b.bin2cn, b.cn_meta,
                                       b.cn_child, b.cn_parent);
   level_begin_kernel<<<grid, 256, 0, s>>>(b.cn_meta, b.sc, b.level_begin);
+  roots_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, b.bin2cn);
 }
 
-void launch_groups(int64_t n, int group_size, Buffers &b, cudaStream_t s) {
+void launch_groups(int64_t n, int group_size, int group_span, Buffers &b, cudaStream_t s) {
   const int grid = grid_for(n, 256, 148 * 16);
   cudaMemsetAsync(b.gflag, 0, n * sizeof(int32_t), s);
-  group_flags_kernel<<<grid, 256, 0, s>>>(b.cn_meta, b.cn_child, b.sc, group_size, b.gflag);
+  group_flags_kernel<<<grid, 256, 0, s>>>(b.cn_meta, b.cn_child, b.cn_parent, b.sc, group_size,
+                                          group_span, b.gflag);
+  system_starts_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, b.gflag);
   int32_t *total = b.counters + 3;
   exclusive_scan(b.gflag, b.gscan, n, nullptr, total, b.scan_tmp, s);
   count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 1);

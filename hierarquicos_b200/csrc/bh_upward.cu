@@ -22,23 +22,21 @@ namespace bh {
 
 namespace {
 
-struct Child {
-  double m, x, y, z;
-};
-
 template <int ORDER>
 __global__ void __launch_bounds__(128)
 upward_level_kernel(int level, const int32_t *__restrict__ level_begin,
                     const int4 *__restrict__ meta, const int32_t *__restrict__ child,
-                    const double4 *__restrict__ spos, const Scalars *__restrict__ sc,
+                    const double4 *__restrict__ spos, const int32_t *__restrict__ sys_of,
+                    const SysScalars *__restrict__ sys,
                     double4 *__restrict__ com, double *__restrict__ quad,
                     double *__restrict__ oct, float4 *__restrict__ fq, float4 *__restrict__ fo) {
   const int lb = level_begin[level], le = level_begin[level + 1];
-  const double inv_m = 1.0 / sc->mass;
-  const double inv_s = 1.0 / sc->ssa;
-  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
   for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x) {
     const int4 mt = meta[j];  // first, count, level, nchild
+    const SysScalars &ss = sys[sys_of[mt.x]];
+    const double inv_m = 1.0 / ss.mass;
+    const double inv_s = 1.0 / ss.ssa;
+    const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
     const bool bucket = (mt.w == 0);
     const int nch = bucket ? mt.y : mt.w;
     // pass 1: mass and centre of mass
@@ -161,15 +159,15 @@ void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s) {
   for (int level = kMaxDepth; level >= 0; --level) {
     if (order >= 8)
       upward_level_kernel<8><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sc, b.cn_com, b.cn_quad, b.cn_oct,
+                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
     else if (order >= 4)
       upward_level_kernel<4><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sc, b.cn_com, b.cn_quad, b.cn_oct,
+                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
     else
       upward_level_kernel<1><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sc, b.cn_com, b.cn_quad, b.cn_oct,
+                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
   }
 }

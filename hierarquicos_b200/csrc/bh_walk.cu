@@ -79,6 +79,8 @@ struct WalkArgs {
   const double4 *spos;
   const int32_t *perm;
   const int32_t *g_first;
+  const int32_t *sys_of;
+  const SysScalars *ss;
   Scalars *sc;
   int32_t *cursor;
   int32_t *stack;
@@ -182,6 +184,16 @@ __device__ __forceinline__ void load_words(const double *p, double (&w)[W]) {
   }
 }
 
+// Reciprocal square root.  FP32: one approximate hardware instruction
+// (rel. error ~2^-22.9) with subnormals flushed: every input is a squared
+// distance in units of the root cube side, never subnormal.  FP64: rsqrt().
+__device__ __forceinline__ float fast_rsqrt(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
+
 // Smallest r^2 of a body pair when there is no softening: a body meets itself
 // (d = 0, contribution exactly 0) and exactly coincident bodies contribute 0;
 // r^-3 stays finite in T.
@@ -196,7 +208,7 @@ __device__ __forceinline__ void body_force(T sx, T sy, T sz, T sm, T rx, T ry, T
   const T dx = sx - rx, dy = sy - ry, dz = sz - rz;
   T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
   if (!SOFT) r2 = max(r2, r2_floor<T>());
-  const T ri = rsqrt(r2);
+  const T ri = fast_rsqrt(r2);
   const T f = (sm * ri) * (ri * ri);
   bx = fma(f, dx, bx); by = fma(f, dy, by); bz = fma(f, dz, bz);
 }
@@ -211,7 +223,7 @@ __device__ __forceinline__ void cell_force(const T *w, T rx, T ry, T rz, T eps2,
                                            T &bz) {
   const T dx = w[0] - rx, dy = w[1] - ry, dz = w[2] - rz;
   const T r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, eps2)));
-  const T rinv = rsqrt(r2);
+  const T rinv = fast_rsqrt(r2);
   const T r2i = rinv * rinv;
   const T r3i = rinv * r2i;
   if (ORDER < 4) {
@@ -264,8 +276,11 @@ struct WalkCounters {
 template <typename T, int ORDER, int TPL, bool SOFT>
 __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER> &S,
                                            int32_t *stack, int stack_cap, int gf, int gn,
-                                           double inv_s, double inv_m, double nq, double no,
-                                           T eps2, T theta2, WalkCounters &wc) {
+                                           const SysScalars &ss, T theta2, WalkCounters &wc) {
+  const double inv_s = 1.0 / ss.ssa, inv_m = 1.0 / ss.mass;
+  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
+  const T eps2 = (T)(a.eps2 * inv_s * inv_s);
+  const int root = ss.root;
   constexpr int W = StageWords<ORDER>::value;
   constexpr bool kKahan = sizeof(T) == 4;
   const int lane = threadIdx.x & (kWarp - 1);
@@ -371,7 +386,8 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
   // looping
   const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
   int64_t group_tests = 0;
-  if (lane == 0) stack[0] = 0;
+  if (root < 0) top = 0;  // a lone body: no tree, no force
+  if (lane == 0) stack[0] = root;
   __syncwarp();
   while (top > 0) {
     if (group_tests > max_tests) { wc.err |= kErrIndex; break; }
@@ -461,20 +477,23 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
   if (ncell > 0) eval_cells(ncell, ncell);
   if (nbody > 0) eval_bodies(nbody, nbody);
 
-  // forces in the original order
-  const double scale = a.G * a.sc->mass * inv_s * inv_s;
+  // forces in the original order; every system's result is an (n_s, 3)
+  // Fortran-ordered block at 3 * off_s
+  const double scale = a.G * ss.mass * inv_s * inv_s;
+  double *out = a.out + 3 * ss.off;
+  const int64_t ns = ss.n;
 #pragma unroll
   for (int t = 0; t < TPL; ++t) {
     if (!valid[t]) continue;
     const int i = gf + lane + kWarp * t;
-    const int p = a.perm[i];
+    const int64_t p = a.perm[i] - ss.off;
     double fxs = (double)ax[t], fys = (double)ay[t], fzs = (double)az[t];
     if (kKahan) { fxs -= (double)cx[t]; fys -= (double)cy[t]; fzs -= (double)cz[t]; }
     double sc = scale;
     if (a.out_kind == 0) sc *= a.spos[i].w;
-    a.out[p] = fxs * sc;
-    a.out[a.n + p] = fys * sc;
-    a.out[2 * a.n + p] = fzs * sc;
+    out[p] = fxs * sc;
+    out[ns + p] = fys * sc;
+    out[2 * ns + p] = fzs * sc;
   }
 }
 
@@ -490,9 +509,6 @@ group_walk_kernel(WalkArgs a) {
   int32_t *stack = a.stack + slot * a.stack_cap;
   const int stack_cap = (int)a.stack_cap;
   const int ngroups = a.sc->n_groups;
-  const double inv_s = 1.0 / a.sc->ssa, inv_m = 1.0 / a.sc->mass;
-  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
-  const T eps2 = (T)(a.eps2 * inv_s * inv_s);
   const T theta2 = (T)a.theta2;
   WalkCounters wc;
   for (;;) {
@@ -502,10 +518,11 @@ group_walk_kernel(WalkArgs a) {
     if (g >= ngroups) break;
     const int gf = a.g_first[g];
     const int gn = a.g_first[g + 1] - gf;
+    const SysScalars &ss = a.ss[a.sys_of[gf]];
     if (MAXTPL == 2 && gn > kWarp)
-      walk_group<T, ORDER, 2, SOFT>(a, S, stack, stack_cap, gf, gn, inv_s, inv_m, nq, no, eps2, theta2, wc);
+      walk_group<T, ORDER, 2, SOFT>(a, S, stack, stack_cap, gf, gn, ss, theta2, wc);
     else
-      walk_group<T, ORDER, 1, SOFT>(a, S, stack, stack_cap, gf, gn, inv_s, inv_m, nq, no, eps2, theta2, wc);
+      walk_group<T, ORDER, 1, SOFT>(a, S, stack, stack_cap, gf, gn, ss, theta2, wc);
   }
   if (wc.err && lane == 0) atomicOr(&a.sc->err, wc.err);
   if (a.count_stats && lane == 0) {
@@ -534,7 +551,6 @@ __global__ void __launch_bounds__(128)
 reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t nt,
                       const int32_t *__restrict__ inv_perm, int64_t *__restrict__ counts) {
   const int L = a.sc->L;
-  const double ssa = a.sc->ssa;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt;
        k += (int64_t)gridDim.x * blockDim.x) {
     if (targets && (targets[k] < 0 || targets[k] >= a.n)) {
@@ -543,6 +559,8 @@ reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t n
       continue;
     }
     const int p = targets ? inv_perm[targets[k]] : (int)k;
+    const SysScalars &ss = a.ss[a.sys_of[p]];
+    const double ssa = ss.ssa;
     const double4 q = a.spos[p];
     const double qp0 = q.x, qp1 = q.y, qp2 = q.z, mp = q.w;
     double fx = 0.0, fy = 0.0, fz = 0.0;
@@ -551,7 +569,7 @@ reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t n
     // level-L lone particle b as ~b - 2^30 (summed at its exact position)
     int32_t st[8 * (kMaxDepth + 2) + 8];
     int top = 0;
-    st[top++] = 0;
+    if (ss.root >= 0) st[top++] = ss.root;
     const int64_t max_pops = (int64_t)a.sc->n_compact + a.n + 8;
     int64_t pops = 0;
     while (top > 0) {
@@ -654,13 +672,14 @@ reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t n
         st[top++] = (ch < 0 && deepest) ? ch - (1 << 30) : ch;
       }
     }
-    const int orig = a.perm[p];
     double sc = 1.0;
     if (a.out_kind == 1) sc = 1.0 / mp;
     if (targets) {
       a.out[k] = fx * sc; a.out[nt + k] = fy * sc; a.out[2 * nt + k] = fz * sc;
     } else {
-      a.out[orig] = fx * sc; a.out[a.n + orig] = fy * sc; a.out[2 * a.n + orig] = fz * sc;
+      double *out = a.out + 3 * ss.off;
+      const int64_t orig = a.perm[p] - ss.off, ns = ss.n;
+      out[orig] = fx * sc; out[ns + orig] = fy * sc; out[2 * ns + orig] = fz * sc;
     }
     if (counts) { counts[2 * k] = npp; counts[2 * k + 1] = npc; }
   }
@@ -690,6 +709,7 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   WalkArgs a;
   a.meta = b.cn_meta; a.child = b.cn_child; a.com = b.cn_com; a.quad = b.cn_quad; a.oct = b.cn_oct;
   a.fq = b.cn_fq; a.fo = b.cn_fo; a.spos = b.spos; a.perm = b.v0; a.g_first = b.g_first;
+  a.sys_of = b.sys_of; a.ss = b.ss;
   a.sc = b.sc; a.cursor = b.counters; a.stack = b.wstack; a.stack_cap = b.wstack_cap;
   a.slots = b.wstack_slots;
   a.stats = b.stats; a.out = out; a.n = n;

@@ -96,6 +96,61 @@ class BHSystem:
                                      C.byref(p), _dptr(out), _stream()))
         return out
 
+    # -- batches of independent systems --
+    def build_batch(self, m, x, y, z, offsets, params: BHParams | None = None,
+                    **kw) -> "BHSystem":
+        """Builds every system of a batch at once.  System s owns entries
+        [offsets[s], offsets[s+1]) of the concatenated m, x, y, z."""
+        dev = torch.device("cuda", self.device)
+        m, x, y, z = (_f64(a, dev) for a in (m, x, y, z))
+        off = _offsets(offsets, m.numel())
+        p = params if params is not None else default_params(**kw)
+        self._inputs = (m, x, y, z)
+        self._offsets = off
+        self.n = m.numel()
+        check(lib().bh_system_build_batch(self._h, _dptr(m), _dptr(x), _dptr(y), _dptr(z),
+                                          off.ctypes.data_as(C.c_void_p), off.size - 1,
+                                          C.byref(p), _stream()))
+        return self
+
+    def forces_batch(self, m, x, y, z, offsets, params: BHParams | None = None, out=None,
+                     **kw) -> torch.Tensor:
+        """Build + walk + sync of a batch; returns the (3N,) float64 device
+        tensor whose entries [3 off_s, 3 off_{s+1}) are system s's SoA forces."""
+        dev = torch.device("cuda", self.device)
+        m, x, y, z = (_f64(a, dev) for a in (m, x, y, z))
+        off = _offsets(offsets, m.numel())
+        p = params if params is not None else default_params(**kw)
+        n = m.numel()
+        if out is None:
+            out = torch.empty(3 * n, dtype=torch.float64, device=dev)
+        self._inputs = (m, x, y, z)
+        self._offsets = off
+        self.n = n
+        check(lib().bh_system_forces_batch(self._h, _dptr(m), _dptr(x), _dptr(y), _dptr(z),
+                                           off.ctypes.data_as(C.c_void_p), off.size - 1,
+                                           C.byref(p), _dptr(out), _stream()))
+        return out
+
+    def batch_info(self) -> dict:
+        nsys = self._offsets.size - 1
+        roots = np.empty(nsys, np.int32)
+        com4 = np.empty((nsys, 4))
+        ssa = np.empty(nsys)
+        check(lib().bh_system_batch_info(self._h, roots.ctypes.data_as(C.c_void_p),
+                                         com4.ctypes.data_as(C.c_void_p),
+                                         ssa.ctypes.data_as(C.c_void_p)))
+        return dict(roots=roots, com=com4[:, :3], mass=com4[:, 3], ssa=ssa)
+
+    def capture(self, params: BHParams, out: torch.Tensor) -> None:
+        """Records build + walk of the current batch (same input tensors,
+        layout and parameters) into a CUDA graph held by the handle."""
+        self._graph_out = out
+        check(lib().bh_system_capture(self._h, C.byref(params), _dptr(out)))
+
+    def replay(self) -> None:
+        check(lib().bh_system_replay(self._h, _stream()))
+
     # -- introspection --
     def info(self) -> dict:
         n, L, nn, ng = C.c_int64(), C.c_int(), C.c_int64(), C.c_int64()
@@ -152,6 +207,18 @@ class BHSystem:
         if counts:
             return f, cnt.view(k, 2).cpu().numpy()
         return f
+
+
+def _offsets(offsets, n: int) -> np.ndarray:
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    if off.ndim != 1 or off.size < 2 or off[0] != 0 or off[-1] != n:
+        raise ValueError("offsets must be [0, ..., N] with N the total number of bodies")
+    return off
+
+
+def offsets_of(sizes) -> np.ndarray:
+    """Batch offsets from the system sizes."""
+    return np.concatenate([[0], np.cumsum(np.asarray(sizes, np.int64))]).astype(np.int64)
 
 
 def direct_targets(m, x, y, z, targets=None, G: float = 1.0, eps: float = 0.0,

@@ -57,11 +57,15 @@ typedef struct bh_params {
                          lies inside it is the reference's sequential centre of mass
                          computed and the build redone when a key differs;
                          2: always run that sequential check; 0: no check          */
-    int reserved[4];
+    int count_stats;  /* 1: the group walk counts its interactions (bh_system_get_stats) */
+    int group_span;   /* target groups: consecutive subtrees of <= group_span bodies are
+                         concatenated in key order and cut into groups of group_size;
+                         0 = 2 * group_size                                         */
+    int reserved[2];
 } bh_params;
 
 /* Defaults: theta 0.5, G 1, eps 0, order 4, forces, depth 21, FP32, amp 1.2,
- * group 64, leaf_cap 8, com_mode 1, strict_keys 1. */
+ * group 64, leaf_cap 8, com_mode 1, strict_keys 1, count_stats 0, group_span 0. */
 void bh_params_default(bh_params *p);
 
 const char *bh_version(void);
@@ -118,6 +122,38 @@ int bh_system_forces(bh_system *sys, const double *d_m, const double *d_x, const
 /* Waits for the stream and turns device-side error flags into a status. */
 int bh_system_sync(bh_system *sys, void *stream);
 
+/* ---- batches of independent systems (no reference counterpart: the
+ *      reference evaluates one system per api_mod.compute_forces call,
+ *      fortran/api3d.f90:20-41, and callers loop over systems) ----
+ * A batch is nsys systems stored back to back in DEVICE arrays: system s owns
+ * entries [offsets[s], offsets[s+1]) of d_m, d_x, d_y, d_z (offsets is a HOST
+ * array of nsys + 1 entries, offsets[0] = 0, strictly increasing).  Every
+ * phase runs once for the whole batch; each system gets its own box, centre
+ * of mass, keys, octree and groups, and its result is the one a build of that
+ * system alone gives (bit for bit).  d_out holds one SoA block per system:
+ * entries [3 offsets[s], 3 offsets[s+1]) are Fx, Fy, Fz of system s (the
+ * (n_s, 3) Fortran array of that system).  depth 0 (automatic) needs nsys 1. */
+int bh_system_build_batch(bh_system *sys, const double *d_m, const double *d_x,
+                          const double *d_y, const double *d_z, const int64_t *offsets,
+                          int nsys, const bh_params *p, void *stream);
+
+/* build_batch + walk + sync. */
+int bh_system_forces_batch(bh_system *sys, const double *d_m, const double *d_x,
+                           const double *d_y, const double *d_z, const int64_t *offsets,
+                           int nsys, const bh_params *p, double *d_out, void *stream);
+
+/* Root node, centre of mass + mass (com4, 4 per system) and root cube side of
+ * every system of the last build, copied to HOST arrays (any may be NULL). */
+int bh_system_batch_info(bh_system *sys, int32_t *roots, double *com4, double *ssa);
+
+/* Records the build and the walk of the current batch (the layout, device
+ * input pointers and sizes of the last build, with the parameters p and
+ * output d_out) into a CUDA graph owned by the handle.  A replay repeats that
+ * work on whatever the input arrays hold then; follow it with bh_system_sync.
+ * A build with another layout or size drops the graph. */
+int bh_system_capture(bh_system *sys, const bh_params *p, double *d_out);
+int bh_system_replay(bh_system *sys, void *stream);
+
 /* After a build: particle count, depth L, compact node count, group count,
  * centre of mass + total mass (com4), root cube side. Synchronises. */
 int bh_system_info(bh_system *sys, int64_t *n, int *depth, int64_t *n_nodes, int64_t *n_groups,
@@ -138,7 +174,7 @@ int bh_system_get_nodes(bh_system *sys, int32_t *meta4, int32_t *child8, int32_t
 /* Group ranges (first sorted particle of each group), n_groups + 1 entries. */
 int bh_system_get_groups(bh_system *sys, int32_t *group_first);
 
-/* Interaction counters of the last walk with counting enabled (reserved[0] = 1
+/* Interaction counters of the last walk with counting enabled (count_stats = 1
  * in bh_params): [0] body-body, [1] body-cell, [2] groups, [3] node tests. */
 int bh_system_get_stats(bh_system *sys, uint64_t *stats4);
 
