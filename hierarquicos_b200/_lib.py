@@ -36,7 +36,7 @@ EXPORTED = [
     "bh_system_get_nodes", "bh_system_get_groups", "bh_system_get_stats",
     "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
     "bh_system_build_batch", "bh_system_forces_batch", "bh_system_batch_info",
-    "bh_system_capture", "bh_system_replay",
+    "bh_system_capture", "bh_system_replay", "bh_kick_drift", "bh_diagnostics",
 ]
 
 BH_NOALLOC_MAX_N = 8192
@@ -111,6 +111,8 @@ def lib():
             "bh_system_batch_info": [_vp, _vp, _vp, _vp],
             "bh_system_capture": [_vp, C.POINTER(BHParams), _vp],
             "bh_system_replay": [_vp, _vp],
+            "bh_kick_drift": [_vp] * 8 + [_vp, _i, _i64, _d, _d, _d, _vp],
+            "bh_diagnostics": [_vp] * 7 + [_vp, _i, _i64, _d, _d, _vp, _vp, _vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

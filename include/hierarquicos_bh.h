@@ -198,6 +198,31 @@ int bh_compute_forces_noalloc(const double *d_m, const double *d_x, const double
                               const double *d_z, int64_t n, const bh_params *p, double *d_out,
                               void *stream);
 
+/* ---- time integration (momentum form, FP64 state; batch layout as above:
+ *      positions, momenta and masses concatenated by system, d_offsets a
+ *      DEVICE copy of the nsys + 1 offsets, forces in the walk's per-system
+ *      (n_s, 3) blocks) ----
+ * For every body: p += kick1 f (skipped when kick1 = 0), p += kick2 f (skipped
+ * when kick2 = 0), then q += (drift p) / m (skipped when drift = 0), with the
+ * reference's operation order and no contraction.  Velocity Verlet
+ * (parareal/parareal.f90:55-63; benchmarks/integration_verlet/integration.f90:
+ * 152-168) is kick_drift(0, dt/2, dt), forces, and at each later step
+ * kick_drift(dt/2, dt/2, dt), with a closing kick_drift(dt/2, 0, 0); the
+ * symplectic Euler coarse step (parareal/parareal.f90:20-35) is
+ * kick_drift(dt, 0, dt) after the forces. */
+int bh_kick_drift(const double *d_m, const double *d_f, double *d_x, double *d_y, double *d_z,
+                  double *d_px, double *d_py, double *d_pz, const int64_t *d_offsets, int nsys,
+                  int64_t n, double kick1, double kick2, double drift, void *stream);
+
+/* Conserved quantities per system (parareal/api3d.f90:108-153, in FP64): d_out
+ * gets 9 doubles per system: total energy, kinetic, potential (softened pair
+ * sum, each pair once), linear momentum (3), angular momentum q x p (3).
+ * d_scratch: 8 n doubles.  O(n_s^2) per system. */
+int bh_diagnostics(const double *d_m, const double *d_x, const double *d_y, const double *d_z,
+                   const double *d_px, const double *d_py, const double *d_pz,
+                   const int64_t *d_offsets, int nsys, int64_t n, double G, double eps,
+                   double *d_scratch, double *d_out, void *stream);
+
 /* FP32 and FP64 fused-multiply-add throughput probe (independent chains,
  * CUDA events): writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64). */
 int bh_probe_fma_peak(int device, double *gflops2);
