@@ -32,13 +32,17 @@ __global__ void __launch_bounds__(256)
 kick_drift_kernel(const double *__restrict__ m, const double *__restrict__ f,
                   double *__restrict__ x, double *__restrict__ y, double *__restrict__ z,
                   double *__restrict__ px, double *__restrict__ py, double *__restrict__ pz,
-                  const int64_t *__restrict__ off, int nsys, int64_t n, double k1, double k2,
-                  double dt) {
+                  const int64_t *__restrict__ off, int nsys, int64_t n, double k1_all,
+                  double k2_all, double dt_all, const double *__restrict__ coef) {
   for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
        g += (int64_t)gridDim.x * blockDim.x) {
     double p0 = px[g], p1 = py[g], p2 = pz[g];
+    const int s = system_of(off, nsys, g);
+    // coefficients of the whole batch, or of each system (coef: 3 per system)
+    const double k1 = coef ? coef[3 * s] : k1_all;
+    const double k2 = coef ? coef[3 * s + 1] : k2_all;
+    const double dt = coef ? coef[3 * s + 2] : dt_all;
     if (k1 != 0.0 || k2 != 0.0) {
-      const int s = system_of(off, nsys, g);
       const int64_t ns = off[s + 1] - off[s], i = g - off[s];
       const double *fs = f + 3 * off[s];
       const double f0 = fs[i], f1 = fs[ns + i], f2 = fs[2 * ns + i];
@@ -149,9 +153,9 @@ diag_reduce_kernel(const double *__restrict__ per_body, const int64_t *__restric
 
 void launch_kick_drift(const double *m, const double *f, double *x, double *y, double *z,
                        double *px, double *py, double *pz, const int64_t *off, int nsys, int64_t n,
-                       double k1, double k2, double dt, cudaStream_t s) {
+                       double k1, double k2, double dt, const double *coef, cudaStream_t s) {
   kick_drift_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(m, f, x, y, z, px, py, pz, off,
-                                                               nsys, n, k1, k2, dt);
+                                                               nsys, n, k1, k2, dt, coef);
 }
 
 void launch_diagnostics(const double *m, const double *x, const double *y, const double *z,
@@ -176,7 +180,21 @@ int bh_kick_drift(const double *d_m, const double *d_f, double *d_x, double *d_y
   if ((kick1 != 0.0 || kick2 != 0.0) && !d_f)
     return bh_report_error(BH_ERR_INVALID, "bh_kick_drift: a kick needs forces");
   bh::launch_kick_drift(d_m, d_f, d_x, d_y, d_z, d_px, d_py, d_pz, d_offsets, nsys, n, kick1,
-                        kick2, drift, (cudaStream_t)stream);
+                        kick2, drift, nullptr, (cudaStream_t)stream);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return bh_report_error(BH_ERR_CUDA, cudaGetErrorString(e));
+  return BH_OK;
+}
+
+int bh_kick_drift_systems(const double *d_m, const double *d_f, double *d_x, double *d_y,
+                          double *d_z, double *d_px, double *d_py, double *d_pz,
+                          const int64_t *d_offsets, int nsys, int64_t n, const double *d_coef,
+                          void *stream) {
+  if (n < 1 || nsys < 1 || !d_offsets || !d_m || !d_x || !d_y || !d_z || !d_px || !d_py ||
+      !d_pz || !d_coef || !d_f)
+    return bh_report_error(BH_ERR_INVALID, "bh_kick_drift_systems: bad arguments");
+  bh::launch_kick_drift(d_m, d_f, d_x, d_y, d_z, d_px, d_py, d_pz, d_offsets, nsys, n, 0.0, 0.0,
+                        0.0, d_coef, (cudaStream_t)stream);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return bh_report_error(BH_ERR_CUDA, cudaGetErrorString(e));
   return BH_OK;

@@ -1,0 +1,396 @@
+"""Serving: a request loop with continuous batching and HBM admission.
+
+Requests are force evaluations or leapfrog integrations (velocity Verlet in
+momentum form, the reference's integrator, benchmarks/integration_verlet/
+integration.f90:110-172) of independent systems of any size.  The server
+keeps every admitted request's particles on the device until it finishes, and
+advances ALL of a lane's active requests together: one tick is one batched
+force evaluation (one build and one walk over all of the lane's systems) and
+one kick-drift launch with per-system coefficients, so a request admitted
+while others are running joins the very next tick.
+
+Design for one GPU:
+  * ``lanes`` independent lanes (default 2), each a host thread with its own
+    engine workspace and CUDA streams.  While one lane waits for its tick's
+    status on the host, the other lane's tick runs on the GPU, so the device
+    stays busy and the lanes' work overlaps.
+  * admission by HBM footprint: a request is admitted (FIFO) when its resident
+    bytes fit in ``hbm_budget`` next to the lanes' fixed workspaces and the
+    requests already resident; otherwise it waits until finished requests
+    release memory.  A request larger than a lane's tick capacity is refused.
+  * inputs arrive in pinned host memory and are copied on a copy stream;
+    results go back on another copy stream, overlapping the next tick.
+  * results do not depend on the mix: every system in a batch gets exactly
+    (bit for bit) the result it gets alone.
+
+Latency of a request = completion of its result copy to the host minus its
+arrival time; ``Server.metrics()`` reports p50/p99 and throughput.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import itertools
+import threading
+import time
+
+import numpy as np
+import torch
+
+from ._lib import BHParams, check, default_params, lib
+from .integrate import as_device
+from .system import BHSystem, _dptr
+
+STATE_BYTES_PER_BODY = 8 + 24 + 24          # m, q, p (FP64)
+RESIDENT_BYTES_PER_BODY = 2 * STATE_BYTES_PER_BODY + 24 + 24  # + tick copy, forces, coefficients
+WORKSPACE_BYTES_PER_BODY = 520              # engine workspace (keys, sort, tree, moments, groups)
+
+_ids = itertools.count()
+
+
+@dataclasses.dataclass(eq=False)
+class Request:
+    """A force evaluation (``kind='force'``) or ``steps`` leapfrog steps of
+    length ``dt`` (``kind='leapfrog'``) of one system.  m (n,), q (n,3),
+    p (n,3) momenta (leapfrog only)."""
+
+    kind: str
+    m: np.ndarray
+    q: np.ndarray
+    p: np.ndarray | None = None
+    steps: int = 0
+    dt: float = 1e-3
+    arrival: float | None = None
+    id: int = dataclasses.field(default_factory=lambda: next(_ids))
+    # filled by the server
+    forces: np.ndarray | None = None     # (n, 3) for force requests
+    q_out: np.ndarray | None = None      # (n, 3) final positions (leapfrog)
+    p_out: np.ndarray | None = None
+    t_admit: float | None = None
+    t_done: float | None = None
+    lane: int = -1
+    error: str | None = None
+
+    def __post_init__(self):
+        if self.kind not in ("force", "leapfrog"):
+            raise ValueError("kind must be 'force' or 'leapfrog'")
+        self.n = int(np.asarray(self.m).size)
+        if self.kind == "leapfrog" and (self.steps < 1 or self.p is None):
+            raise ValueError("a leapfrog request needs momenta and steps >= 1")
+        self._done = threading.Event()
+        self._evals = 0  # force evaluations done
+
+    @property
+    def evals_needed(self) -> int:
+        return 1 if self.kind == "force" else self.steps + 1
+
+    @property
+    def latency(self) -> float | None:
+        return None if self.t_done is None else self.t_done - self.arrival
+
+    def wait(self, timeout=None) -> bool:
+        return self._done.wait(timeout)
+
+
+class _Lane:
+    def __init__(self, server: "Server", index: int):
+        self.server = server
+        self.index = index
+        dev = server.device
+        with torch.cuda.device(dev):
+            self.stream = torch.cuda.Stream(dev)
+            self.h2d = torch.cuda.Stream(dev)
+            self.d2h = torch.cuda.Stream(dev)
+        self.sys = BHSystem(dev.index)
+        self.active: list[Request] = []
+        self.state: dict[int, dict] = {}
+        self.done_q: collections.deque = collections.deque()
+        self.done_cv = threading.Condition()
+        self.ticks = 0
+        self.tick_bodies = 0
+        self.thread = threading.Thread(target=self._run, name=f"bh-lane-{index}", daemon=True)
+        self.finisher = threading.Thread(target=self._finish_loop, name=f"bh-done-{index}",
+                                         daemon=True)
+
+    # -- staging --
+    def _stage(self, r: Request):
+        dev = self.server.device
+        host = r._pinned
+        with torch.cuda.stream(self.h2d):
+            d = {k: v.to(dev, non_blocking=True) for k, v in host.items()}
+            ev = torch.cuda.Event()
+            ev.record(self.h2d)
+        self.stream.wait_event(ev)
+        for v in d.values():
+            v.record_stream(self.stream)
+        self.state[r.id] = d
+
+    # -- one tick: forces of every active system, then the per-system kicks --
+    def _tick(self):
+        srv = self.server
+        act = self.active
+        dev = srv.device
+        sizes = [r.n for r in act]
+        off = np.zeros(len(act) + 1, np.int64)
+        off[1:] = np.cumsum(sizes)
+        n = int(off[-1])
+        with torch.cuda.stream(self.stream):
+            st = [self.state[r.id] for r in act]
+            cat = {k: torch.cat([s[k] for s in st]) for k in ("m", "x", "y", "z", "px", "py", "pz")}
+            out = torch.empty(3 * n, dtype=torch.float64, device=dev)
+            self.sys.forces_batch(cat["m"], cat["x"], cat["y"], cat["z"], off, srv.params, out=out)
+            coef = np.zeros((len(act), 3))
+            for i, r in enumerate(act):
+                if r.kind == "leapfrog":
+                    h = 0.5 * r.dt
+                    k = r._evals
+                    coef[i] = (0.0, h, r.dt) if k == 0 else ((h, h, r.dt) if k < r.steps
+                                                             else (h, 0.0, 0.0))
+                r._evals += 1
+            if any(r.kind == "leapfrog" for r in act):
+                d_coef = torch.as_tensor(coef.ravel(), device=dev)
+                d_off = torch.as_tensor(off, device=dev)
+                check(lib().bh_kick_drift_systems(
+                    _dptr(cat["m"]), _dptr(out), _dptr(cat["x"]), _dptr(cat["y"]),
+                    _dptr(cat["z"]), _dptr(cat["px"]), _dptr(cat["py"]), _dptr(cat["pz"]),
+                    _dptr(d_off), len(act), n, _dptr(d_coef), self.stream.cuda_stream))
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        keep = []
+        finished = []
+        for i, r in enumerate(act):
+            a, b = int(off[i]), int(off[i + 1])
+            self.state[r.id] = {k: v[a:b] for k, v in cat.items()}
+            if r._evals >= r.evals_needed:
+                finished.append((r, a, b))
+            else:
+                keep.append(r)
+        if finished:
+            self.d2h.wait_event(ev)
+            with torch.cuda.stream(self.d2h):
+                for r, a, b in finished:
+                    if r.kind == "force":
+                        r._host_out["f"].copy_(out[3 * a:3 * b], non_blocking=True)
+                    else:
+                        for k in ("x", "y", "z", "px", "py", "pz"):
+                            r._host_out[k].copy_(cat[k][a:b], non_blocking=True)
+                    done = torch.cuda.Event()
+                    done.record(self.d2h)
+                    out.record_stream(self.d2h)
+                    for v in cat.values():
+                        v.record_stream(self.d2h)
+                    with self.done_cv:
+                        self.done_q.append((r, done))
+                        self.done_cv.notify()
+        for r, _, _ in finished:
+            del self.state[r.id]
+        self.active = keep
+        self.ticks += 1
+        self.tick_bodies += n
+
+    def _run(self):
+        srv = self.server
+        torch.cuda.set_device(srv.device)
+        try:
+            while True:
+                new = srv._admit(self)
+                for r in new:
+                    self._stage(r)
+                self.active.extend(new)
+                if not self.active:
+                    if srv._stopping and srv._idle():
+                        break
+                    with srv._cv:
+                        srv._cv.wait(0.01)
+                    continue
+                self._tick()
+        except Exception as e:  # a failed tick fails its requests, not the server
+            for r in self.active:
+                r.error = str(e)
+                r.t_done = time.perf_counter()
+                srv._release(r)
+                r._done.set()
+            self.active = []
+            srv._lane_error = e
+        finally:
+            with self.done_cv:
+                self.done_q.append(None)
+                self.done_cv.notify()
+
+    def _finish_loop(self):
+        torch.cuda.set_device(self.server.device)
+        while True:
+            with self.done_cv:
+                while not self.done_q:
+                    self.done_cv.wait()
+                item = self.done_q.popleft()
+            if item is None:
+                return
+            r, ev = item
+            ev.synchronize()
+            r.t_done = time.perf_counter()
+            ho = r._host_out
+            if r.kind == "force":
+                r.forces = ho["f"].numpy().reshape(3, r.n).T
+            else:
+                r.q_out = np.stack([ho["x"].numpy(), ho["y"].numpy(), ho["z"].numpy()], axis=1)
+                r.p_out = np.stack([ho["px"].numpy(), ho["py"].numpy(), ho["pz"].numpy()], axis=1)
+            self.server._release(r)
+            r._done.set()
+
+
+class Server:
+    """Continuous-batching force server on one GPU.
+
+    ``params``: engine parameters (theta, eps, order, ...; default theta 0.5,
+    quadrupole).  ``hbm_budget``: bytes the server may hold on the device.
+    ``max_tick_bodies``: bodies of one lane's tick (bounds the lanes'
+    workspaces and a tick's latency)."""
+
+    def __init__(self, params: BHParams | None = None, device=None, hbm_budget: float = 150e9,
+                 max_tick_bodies: int = 1 << 23, lanes: int = 2, **kw):
+        self.device = as_device(device)
+        self.params = params if params is not None else default_params(**kw)
+        self.hbm_budget = float(hbm_budget)
+        self.max_tick_bodies = int(max_tick_bodies)
+        self.workspace_bytes = lanes * WORKSPACE_BYTES_PER_BODY * self.max_tick_bodies
+        if self.workspace_bytes >= self.hbm_budget:
+            raise ValueError("hbm_budget does not cover the lanes' workspaces")
+        self._cv = threading.Condition()
+        self._pending: collections.deque[Request] = collections.deque()
+        self._resident = 0
+        self.max_resident = 0
+        self._stopping = False
+        self._inflight = 0
+        self._lane_error = None
+        self.completed: list[Request] = []
+        self.lanes = [_Lane(self, i) for i in range(lanes)]
+        self._lane_bodies = [0] * lanes
+        self._started = False
+
+    @staticmethod
+    def footprint(n: int) -> int:
+        """Device bytes a request of n bodies holds while it is resident."""
+        return RESIDENT_BYTES_PER_BODY * n
+
+    # -- client side --
+    def submit(self, r: Request) -> Request:
+        if r.n > self.max_tick_bodies:
+            raise ValueError(f"request of {r.n} bodies exceeds a lane's tick ({self.max_tick_bodies})")
+        if self.footprint(r.n) > self.hbm_budget - self.workspace_bytes:
+            raise ValueError("request larger than the HBM budget")
+        self._pin(r)
+        if r.arrival is None:
+            r.arrival = time.perf_counter()
+        with self._cv:
+            self._pending.append(r)
+            self._inflight += 1
+            self._cv.notify_all()
+        return r
+
+    @staticmethod
+    def _pin(r: Request):
+        def pin(a):
+            t = torch.empty(len(a), dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = a
+            return t
+
+        m = np.asarray(r.m, np.float64)
+        q = np.asarray(r.q, np.float64)
+        host = {"m": pin(m), "x": pin(q[:, 0]), "y": pin(q[:, 1]), "z": pin(q[:, 2])}
+        if r.kind == "leapfrog":
+            p = np.asarray(r.p, np.float64)
+            host.update(px=pin(p[:, 0]), py=pin(p[:, 1]), pz=pin(p[:, 2]))
+            r._host_out = {k: torch.empty(r.n, dtype=torch.float64, pin_memory=True)
+                           for k in ("x", "y", "z", "px", "py", "pz")}
+        else:
+            z = torch.zeros(r.n, dtype=torch.float64, pin_memory=True)
+            host.update(px=z, py=z, pz=z)
+            r._host_out = {"f": torch.empty(3 * r.n, dtype=torch.float64, pin_memory=True)}
+        r._pinned = host
+
+    def start(self) -> "Server":
+        if not self._started:
+            self._started = True
+            for ln in self.lanes:
+                ln.thread.start()
+                ln.finisher.start()
+        return self
+
+    def drain(self, timeout: float | None = None) -> None:
+        """Waits until every submitted request has finished."""
+        t_end = None if timeout is None else time.perf_counter() + timeout
+        with self._cv:
+            while self._inflight > 0:
+                if self._lane_error is not None:
+                    raise RuntimeError(f"lane failed: {self._lane_error}")
+                left = None if t_end is None else t_end - time.perf_counter()
+                if left is not None and left <= 0:
+                    raise TimeoutError("requests still running")
+                self._cv.wait(0.05 if left is None else min(0.05, left))
+
+    def stop(self) -> None:
+        with self._cv:
+            self._stopping = True
+            self._cv.notify_all()
+        for ln in self.lanes:
+            if ln.thread.is_alive():
+                ln.thread.join()
+            if ln.finisher.is_alive():
+                ln.finisher.join()
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *a):
+        self.stop()
+
+    # -- lane side --
+    def _idle(self) -> bool:
+        return not self._pending
+
+    def _admit(self, lane: _Lane) -> list[Request]:
+        """FIFO admission of pending requests into this lane while they fit the
+        HBM budget and the lane's tick capacity."""
+        out = []
+        with self._cv:
+            room = self.hbm_budget - self.workspace_bytes
+            bodies = sum(r.n for r in lane.active)
+            while self._pending:
+                r = self._pending[0]
+                fp = self.footprint(r.n)
+                if self._resident + fp > room or bodies + r.n > self.max_tick_bodies:
+                    break
+                self._pending.popleft()
+                self._resident += fp
+                self.max_resident = max(self.max_resident, self._resident)
+                bodies += r.n
+                r.t_admit = time.perf_counter()
+                r.lane = lane.index
+                out.append(r)
+        return out
+
+    def _release(self, r: Request):
+        with self._cv:
+            self._resident -= self.footprint(r.n)
+            self._inflight -= 1
+            self.completed.append(r)
+            self._cv.notify_all()
+
+    # -- reporting --
+    def metrics(self, requests=None) -> dict:
+        rs = [r for r in (requests if requests is not None else self.completed)
+              if r.t_done is not None and r.error is None]
+        if not rs:
+            return {}
+        lat = np.array([r.latency for r in rs]) * 1e3
+        t0 = min(r.arrival for r in rs)
+        t1 = max(r.t_done for r in rs)
+        forces = sum(r.n * r.evals_needed for r in rs)
+        return {"requests": len(rs), "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "wall_s": t1 - t0, "forces": int(forces), "forces_per_s": forces / (t1 - t0),
+                "ticks": sum(ln.ticks for ln in self.lanes),
+                "mean_tick_bodies": sum(ln.tick_bodies for ln in self.lanes)
+                / max(1, sum(ln.ticks for ln in self.lanes)),
+                "max_resident_bytes": self.max_resident}

@@ -214,6 +214,14 @@ int bh_kick_drift(const double *d_m, const double *d_f, double *d_x, double *d_y
                   double *d_px, double *d_py, double *d_pz, const int64_t *d_offsets, int nsys,
                   int64_t n, double kick1, double kick2, double drift, void *stream);
 
+/* bh_kick_drift with coefficients per system: d_coef (DEVICE) holds kick1,
+ * kick2, drift for each of the nsys systems (all zero: the system is left as
+ * it is).  One launch advances systems at different stages of their steps. */
+int bh_kick_drift_systems(const double *d_m, const double *d_f, double *d_x, double *d_y,
+                          double *d_z, double *d_px, double *d_py, double *d_pz,
+                          const int64_t *d_offsets, int nsys, int64_t n, const double *d_coef,
+                          void *stream);
+
 /* Conserved quantities per system (parareal/api3d.f90:108-153, in FP64): d_out
  * gets 9 doubles per system: total energy, kinetic, potential (softened pair
  * sum, each pair once), linear momentum (3), angular momentum q x p (3).
