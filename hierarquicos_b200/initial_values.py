@@ -201,3 +201,33 @@ def generate_initial_values(N: int, size_qs: float = -1.0, size_ps: float = -1.0
     com = (m[:, None] * qs).sum(axis=0) / m.sum()
     qs = qs - com
     return m, np.ascontiguousarray(qs), np.ascontiguousarray(ps)
+
+
+PROFILES = {"uniform": 0, "uniform_sphere": 1, "plummer": 2, "homogeneous": 3, "hernquist": 4}
+
+
+def generate_initial_values_device(N: int, size_qs: float = -1.0, size_ps: float = -1.0,
+                                   nm: bool = True, td: bool = False, pr: str = "plummer",
+                                   pp=(1.0, 1.0), seed: int = 0, velocities: bool = True,
+                                   device=None):
+    """The same distributions as ``generate_initial_values``, drawn on the GPU
+    by ``bh_generate_ics`` (counter-based streams, so not the host's draws).
+    Returns CUDA tensors m (N,), q (3, N), p (3, N) (rows x, y, z)."""
+    import ctypes as C
+
+    import torch
+
+    from ._lib import check, lib
+
+    if pr not in PROFILES:
+        raise ValueError(f'Unknow density profile: "{pr}"')
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    m = torch.empty(N, dtype=torch.float64, device=dev)
+    q = torch.empty(3, N, dtype=torch.float64, device=dev)
+    p = torch.empty(3, N, dtype=torch.float64, device=dev)
+    scratch = torch.empty(2400, dtype=torch.float64, device=dev)
+    check(lib().bh_generate_ics(PROFILES[pr], N, float(size_qs), float(size_ps), int(td), int(nm),
+                                float(pp[0]), float(pp[1]), C.c_uint64(seed & (2**64 - 1)),
+                                int(velocities), m.data_ptr(), q.data_ptr(), p.data_ptr(),
+                                scratch.data_ptr(), torch.cuda.current_stream(dev).cuda_stream))
+    return m, q, p

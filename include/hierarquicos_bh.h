@@ -231,6 +231,19 @@ int bh_diagnostics(const double *d_m, const double *d_x, const double *d_y, cons
                    const int64_t *d_offsets, int nsys, int64_t n, double G, double eps,
                    double *d_scratch, double *d_out, void *stream);
 
+/* ---- initial conditions on the device (initial_values/initial_values.f90:
+ *      51-381; plummer.f90, hernquist.f90, homogeneous.f90) ----
+ * profile: 0 uniform cube, 1 uniform sphere, 2 Plummer, 3 homogeneous sphere,
+ * 4 Hernquist; par: b, R or a; size_qs >= 0 truncates radii (rejection),
+ * size_ps >= 0 bounds the speeds; nm 1 equal masses 1/n, 0 random masses
+ * summing to 1; two_d zeroes z.  Writes d_m (n), d_q and d_p (SoA, 3 n:
+ * x block, y block, z block; momenta p = m v) with the centre of mass and the
+ * total momentum at zero.  Counter-based streams: the result depends only on
+ * the seed and n.  d_scratch: 2400 doubles.  Synchronous. */
+int bh_generate_ics(int profile, int64_t n, double size_qs, double size_ps, int two_d, int nm,
+                    double G, double par, uint64_t seed, int velocities, double *d_m,
+                    double *d_q, double *d_p, double *d_scratch, void *stream);
+
 /* FP32 and FP64 fused-multiply-add throughput probe (independent chains,
  * CUDA events): writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64). */
 int bh_probe_fma_peak(int device, double *gflops2);
