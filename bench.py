@@ -1,24 +1,43 @@
 #!/usr/bin/env python
 """Benchmark of the Barnes-Hut force path on B200.
 
-Workload (one step = one full force evaluation: keys -> radix sort -> octree
--> multipoles -> groups -> walk): Hernquist sphere, N = 1,048,576, a = 1,
-truncated at 100 a, equal masses, seeded; theta = 0.5, quadrupole, softening
-0.01, FP32 Kahan-compensated group walk.  The metric is forces/s; the error
-of every run against the FP64 direct sum is measured on 16,384 seeded targets.
+Headline (default): force evaluations of N = 1,048,576-body Hernquist systems
+(a = 1, truncated at 100 a, equal masses, seeded; theta = 0.5, quadrupole,
+softening 0.01, FP32 Kahan-compensated group walk), served by the continuous
+batching server against the plain single-system call:
+
+  * plain  -- ``bh_system_forces`` per system (keys -> radix sort -> octree ->
+    multipoles -> groups -> walk -> status), device-resident inputs, the L2
+    flushed before every call;
+  * served -- the same systems submitted at once to ``serving.Server``
+    (2 lanes, continuous batching), device-resident requests; p50/p99 latency
+    per request;
+  * e2e    -- both again from pinned HOST buffers with the copies included:
+    plain through ``bh_compute_forces_ex`` (the api3d drop-in), served with
+    host requests;
+  * batched -- 512 independent systems (N log-uniform in [1024, 65536], Plummer
+    and uniform-density spheres): one batched build + walk (and its CUDA-graph
+    replay) with autotuned group/leaf parameters against a loop of plain
+    calls.
+
+The RMS relative error is measured against the FP64 direct sum on 16,384
+seeded targets; served results are checked equal (bit for bit) to the plain
+ones.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One process per GPU (torchrun for N > 1): every rank evaluates its own
-independent system (weak scaling, no collective on the data path); times are
-the max over ranks.  ``--impl reference`` times the CPU restatement of the
-reference's Fortran (the reference cannot be compiled here: no Fortran
-compiler) on this host's cores.
+One process per GPU (torchrun for N > 1): every rank serves its own systems
+(weak scaling, no collective on the data path); times are the max over
+ranks.  ``--impl reference`` times the CPU restatement of the reference's
+Fortran (the reference cannot be compiled here: no Fortran compiler) on this
+host's cores.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -36,7 +55,7 @@ THETA, EPS, ORDER = 0.5, 0.01, 4
 N_ERR_TARGETS = 16384
 FLOPS_PP = 20          # body-body (GPU Gems 3 convention), morton_octree.f90:676-686
 FLOPS_PC = {1: 20, 4: 60, 8: 140}  # cell terms, octree_default.f90:1993-2083
-METRIC = "forces/s (N=1M, theta=0.5, err<=1e-3 vs FP64)"
+METRIC = "forces/s (N=1M, theta=0.5, err<=1e-3 vs FP64): served vs plain; p50/p99 ms"
 
 
 def parse():
@@ -50,8 +69,11 @@ def parse():
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--leaf-cap", type=int, default=8)
+    ap.add_argument("--group-span", type=int, default=0)
+    ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--no-extras", action="store_true",
-                    help="timed steps only (no error check, e2e, probe or CPU baseline)")
+                    help="plain timed calls only (no serving, error check, e2e, batch or CPU baseline)")
     return ap.parse_args()
 
 
@@ -63,12 +85,13 @@ def workload(n, seed):
     return m, q
 
 
-def config(args, world):
-    return {"workload": f"hernquist N={args.n} a=1 r<=100a equal masses seeded",
-            "n_per_gpu": args.n, "theta": THETA, "eps": EPS, "order": args.order,
-            "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk", 2: "fp64 per-target"}[args.precision],
-            "group_size": args.group_size, "leaf_cap": args.leaf_cap, "keys": "63-bit, strict",
-            "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"independent systems x{world}"}
+def device_workload(n, seed):
+    """Hernquist system drawn on the device: m, x, y, z (n,) CUDA tensors."""
+    from hierarquicos_b200.initial_values import generate_initial_values_device
+
+    m, q, _ = generate_initial_values_device(n, 100.0, -1.0, True, False, "hernquist", (1.0, 1.0),
+                                             seed=seed, velocities=False)
+    return m, q[0].contiguous(), q[1].contiguous(), q[2].contiguous()
 
 
 class ClockSampler:
@@ -80,47 +103,44 @@ class ClockSampler:
 
     def __init__(self, gpu):
         self.gpu = gpu
-        self.proc = None
-        self.lines = []
+        self.rows = []
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
-        except Exception:
-            self.proc = None
+        except OSError:
+            self.p = None
         return self
 
     def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        for line in self.p.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *a):
-        if self.proc:
+        if self.p is not None:
             time.sleep(0.25)
-            self.proc.terminate()
+            self.p.terminate()
             try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
 
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        for r in self.rows:
             try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
@@ -128,20 +148,37 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def gpu_launches_per_step(n, order, strict=True):
-    """Kernel launches of one build + walk (counted from the pipeline)."""
-    sort_tiles = (n + 4095) // 4096
-    scan = 3
-    particle_sort = 8 * (1 + scan + 1)          # 8 passes: upsweep, scan x3, downsweep
-    first_bits = int(np.ceil(np.log2(n + 1))) + 1
-    node_sort = ((first_bits + 5 + 7) // 8) * (1 + scan + 1)
-    keys = 3 + (1 if strict else 0)             # reduce, finalize, keys (+ sequential COM)
-    tree = 2 + scan + 1 + 1 + node_sort + 1 + 1 + 1   # karras, mark, scan, count, keys, sort, bin2cn, records, levels
+def launches_per_evaluation(n, nsys=1, L=21):
+    """Our kernel launches in one build + walk (the pipeline's launch sequence;
+    the ncu launch list shows 105 for one system of 2^20 bodies)."""
+    scan = 3                                           # reduce, block scan, apply
+    sort_pass = 1 + scan + 1                           # upsweep, scan, downsweep
+    keys = 3                                           # reduce, finalize, keys
+    particle_sort = math.ceil(3 * L / 8) * sort_pass
+    by_system = 0
+    if nsys >= 2:
+        by_system = 1 + math.ceil(max(1, math.ceil(math.log2(nsys))) / 8) * sort_pass + 1
+    first_bits = 1
+    while (1 << first_bits) <= n:
+        first_bits += 1
+    node_sort = math.ceil((first_bits + 5) / 8) * sort_pass
+    # karras, mark, scan, count, compact keys, node sort, bin2cn, records, levels, roots
+    tree = 2 + scan + 1 + 1 + node_sort + 1 + 1 + 1 + 1
     upward = 22
-    groups = 1 + scan + 1 + 1                   # flags, scan, count, first
-    walk = 1 + (1 if strict else 0)             # walk (+ key verification)
-    del sort_tiles
-    return keys + particle_sort + 1 + tree + upward + groups + walk
+    groups = 1 + 1 + scan + 1 + 1                      # flags, starts, scan, count, first
+    walk = 1
+    return keys + particle_sort + by_system + 1 + tree + upward + groups + walk
+
+
+def dist_max(x, dev, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_ours(args):
@@ -160,84 +197,153 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
     n = args.n
-    m, q = workload(n, seed=1000 + rank)
-    tm = torch.as_tensor(m, device=dev)
-    tx, ty, tz = (torch.as_tensor(np.ascontiguousarray(q[:, k]), device=dev) for k in range(3))
-    out = torch.empty(3 * n, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    K, W = args.steps, args.warmup
     p = _lib.default_params(theta=THETA, eps=EPS, order=args.order, precision=args.precision,
-                            group_size=args.group_size, leaf_cap=args.leaf_cap)
-    sysm = BHSystem(local)
+                            group_size=args.group_size, leaf_cap=args.leaf_cap,
+                            group_span=args.group_span)
     stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def step():
-        sysm.build(tm, tx, ty, tz, p)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e1.record(stream)
-        sysm.walk(p, out)
-        return e1
+    # K timed + W warm-up systems, drawn on the device
+    systems = [device_workload(n, seed=1000 + 97 * rank + i) for i in range(K + W)]
+    out = torch.empty(3 * n, dtype=torch.float64, device=dev)
 
-    for _ in range(args.warmup):
-        step()
-        sysm.sync()
+    # ---- plain: one call per system ----
+    sysm = BHSystem(local)
+    for i in range(W):
+        sysm.forces(*systems[K + i], p, out=out)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     t_total, t_build, t_walk = [], [], []
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
+        for i in range(K):
             flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e2 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            e1 = step()
-            e2.record(stream)
-            sysm.sync()
-            t_total.append(e0.elapsed_time(e2))
-            t_build.append(e0.elapsed_time(e1))
-            t_walk.append(e1.elapsed_time(e2))
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
+            sysm.build(*systems[i], p)
+            ev[1].record(stream)
+            sysm.walk(p, out)
+            ev[2].record(stream)
+            sysm.sync()          # status, strict-key check (and its rare rebuild)
+            ev[3].record(stream)
+            ev[3].synchronize()
+            t_total.append(ev[0].elapsed_time(ev[3]))
+            t_build.append(ev[0].elapsed_time(ev[1]))
+            t_walk.append(ev[1].elapsed_time(ev[2]))
         torch.cuda.synchronize()
-    sum_ms = float(sum(t_total))
-    if world > 1:
-        tt = torch.tensor([sum_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        sum_ms = float(tt.item())
-        dist.barrier()
-    ms_per_step = sum_ms / args.steps
-    value = world * n * args.steps / (sum_ms * 1e-3)
+    plain_ms = dist_max(float(sum(t_total)), dev, world) / K
+    plain_value = world * n / (plain_ms * 1e-3)
+    f_plain_last = out.clone()
 
-    line = {"metric": METRIC, "value": value, "unit": "forces/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 walk (Kahan), f64 keys/moments", "data": "synthetic (seeded Hernquist ICs)",
-            "config": config(args, world), "clocks": clocks.summary(),
-            "phases_ms": {"build": statistics.mean(t_build), "walk": statistics.mean(t_walk)},
-            "gpu_launches": gpu_launches_per_step(n, args.order) * args.steps}
+    line = {"metric": METRIC, "value": plain_value, "unit": "forces/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": plain_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 walk (Kahan), f64 keys/moments",
+            "data": "synthetic (seeded Hernquist ICs drawn on the device)",
+            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, force requests",
+                       "n_per_request": n, "requests_per_gpu": K, "theta": THETA, "eps": EPS,
+                       "order": args.order,
+                       "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk",
+                                2: "fp64 per-target"}[args.precision],
+                       "group_size": args.group_size, "leaf_cap": args.leaf_cap,
+                       "group_span": args.group_span or 2 * args.group_size, "keys": "63-bit, strict",
+                       "l2": "plain: flushed (256 MiB write) before every call; served: every request "
+                             "touches > 500 MB of distinct data (inputs larger than L2)",
+                       "parallelism": f"independent systems per rank x{world}"},
+            "plain": {"value": plain_value, "unit": "forces/s", "ms_per_step": plain_ms,
+                      "phases_ms": {"build": statistics.mean(t_build),
+                                    "walk": statistics.mean(t_walk),
+                                    "status": statistics.mean(t_total) - statistics.mean(t_build)
+                                    - statistics.mean(t_walk)}},
+            "clocks": clocks.summary(),
+            "gpu_launches": launches_per_evaluation(n) * K}
 
     if not args.no_extras:
-        # accuracy against the FP64 direct sum on seeded targets
+        from hierarquicos_b200 import serving
+
+        def serve(reqs, warm):
+            """Submits ``warm`` and waits, then submits all of ``reqs`` at
+            once; returns (device ms from first submission to the last result,
+            metrics of ``reqs``)."""
+            with serving.Server(p, device=local, lanes=args.lanes, max_tick_bodies=2 * n,
+                                hbm_budget=150e9) as srv:
+                for r in warm:
+                    srv.submit(r)
+                srv.drain(timeout=600)
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                for ln in srv.lanes:
+                    ln.ticks = ln.tick_bodies = 0
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                t0 = time.perf_counter()
+                for r in reqs:
+                    r.arrival = t0
+                    srv.submit(r)
+                srv.drain(timeout=600)
+                torch.cuda.synchronize()
+                b.record(stream)
+                b.synchronize()
+                return a.elapsed_time(b), srv.metrics(reqs)
+
+        def dev_reqs(idx):
+            return [serving.Request("force", systems[i][0], torch.stack(systems[i][1:4]))
+                    for i in idx]
+
+        # ---- served: the same K systems as device-resident requests ----
+        reqs = dev_reqs(range(K))
+        with ClockSampler(local) as sclocks:
+            served_total_ms, met = serve(reqs, dev_reqs(range(K, K + W)))
+        served_ms = dist_max(served_total_ms, dev, world) / K
+        served_value = world * n / (served_ms * 1e-3)
+        # a request served in a two-system tick equals the plain call, bit for bit
+        same = bool(torch.equal(reqs[-1].forces.T.reshape(-1), f_plain_last))
+        line["value"] = served_value
+        line["ms_per_step"] = served_ms
+        line["served"] = {"value": served_value, "unit": "forces/s", "ms_per_request": served_ms,
+                          "p50_ms": met["p50_ms"], "p99_ms": met["p99_ms"], "ticks": met["ticks"],
+                          "mean_tick_bodies": met["mean_tick_bodies"], "lanes": args.lanes,
+                          "equal_to_plain_bitwise": same}
+        line["served_over_plain"] = served_value / plain_value
+        line["latency_ms"] = {"p50": met["p50_ms"], "p99": met["p99_ms"],
+                              "definition": "all K requests arrive at once; arrival to result ready "
+                                            "on the device"}
+        line["clocks"] = sclocks.summary()
+        line["clocks_plain"] = clocks.summary()
+        line["gpu_launches"] = launches_per_evaluation(2 * n, 2) * met["ticks"]
+
+        # ---- accuracy against the FP64 direct sum (plain output of the last system) ----
+        mK, xK, yK, zK = systems[K - 1]
         rng = np.random.default_rng(12345 + rank)
         tg = np.sort(rng.choice(n, N_ERR_TARGETS, replace=False))
         ttg = torch.as_tensor(tg, device=dev)
-        fd = direct_targets(tm, tx, ty, tz, ttg, 1.0, EPS).T.cpu().numpy()
-        f = out.view(3, n).T[ttg].cpu().numpy()
-        err = error_stats(f, fd, m[tg], q[tg])
-        # reference-semantics interaction counts on the same targets
+        fd = direct_targets(mK, xK, yK, zK, ttg, 1.0, EPS).T.cpu().numpy()
+        f = f_plain_last.view(3, n).T[ttg].cpu().numpy()
+        mh = mK.cpu().numpy()
+        qh = torch.stack([xK, yK, zK], 1).cpu().numpy()
+        err = error_stats(f, fd, mh[tg], qh[tg])
+        sysm.build(mK, xK, yK, zK, p)
+        sysm.sync()
         fr, cnt = sysm.reference_targets(tg, p, counts=True)
         err_ref = error_stats(fr, fd)
         mean_pp, mean_pc = cnt.mean(axis=0)
         line["accuracy"] = {"targets": N_ERR_TARGETS, "rms_rel": err["rms_rel"],
                             "max_rel": err["max_rel"], "normalised_rms": err.get("normalised_rms"),
                             "reference_walk_rms_rel": err_ref["rms_rel"],
-                            "meets_1e-3": err["rms_rel"] <= 1e-3}
-        # executed interactions of the group walk
+                            "meets_1e-3": err["rms_rel"] <= 1e-3,
+                            "served": "identical to plain (bitwise)" if same else "DIFFERS"}
+
+        # ---- roofline of the walk (dominant kernel) ----
         p.count_stats = 1
         sysm.walk(p, out)
         sysm.sync()
         st = sysm.stats()
         p.count_stats = 0
         peak = np.zeros(2)
-        _lib.check(_lib.lib().bh_probe_fma_peak(local, peak.ctypes.data_as(__import__("ctypes").c_void_p)))
+        _lib.check(_lib.lib().bh_probe_fma_peak(local, peak.ctypes.data_as(C.c_void_p)))
         alg_flops = n * (mean_pp * FLOPS_PP + mean_pc * FLOPS_PC[args.order])
         exe_flops = float(st[0]) * FLOPS_PP + float(st[1]) * FLOPS_PC[args.order]
         t_w = statistics.mean(t_walk) * 1e-3
@@ -246,39 +352,37 @@ def run_ours(args):
         tf = os.path.join(ROOT, "profiles", "walk_dram_traffic.json")
         if os.path.exists(tf):
             with open(tf) as fh:
-                tj = json.load(fh)
-            traffic = tj.get("bytes_per_launch_scaled")
-        line["roofline"] = {"bound": "fp32", "kernel": "group_walk_kernel", "achieved": achieved,
-                            "peak": peak[0] / 1e3, "unit": "TFLOP/s", "frac": achieved / (peak[0] / 1e3),
-                            "traffic": traffic,
-                            "peak_source": "measured FP32 FMA probe in this run (MEASURED_PEAKS.json has no FP32 figure)",
-                            "algorithmic_flops_per_launch": alg_flops,
-                            "executed_flops_per_launch": exe_flops,
-                            "reference_interactions_per_target": {"body_body": float(mean_pp), "body_cell": float(mean_pc)},
-                            "executed_interactions_per_target": {"body_body": float(st[0]) / n, "body_cell": float(st[1]) / n},
-                            "walk_ms": t_w * 1e3, "fp64_peak_tflops": peak[1] / 1e3}
-        # end to end through the public host API, pinned host buffers
-        hm = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        hx = torch.empty_like(hm)
-        hy = torch.empty_like(hm)
-        hz = torch.empty_like(hm)
-        hout = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
-        hm.numpy()[:] = m
-        hx.numpy()[:] = q[:, 0]
-        hy.numpy()[:] = q[:, 1]
-        hz.numpy()[:] = q[:, 2]
-        import ctypes as C
+                traffic = json.load(fh).get("bytes_per_launch_scaled")
+        line["roofline"] = {
+            "bound": "fp32", "kernel": "group_walk_kernel", "achieved": achieved,
+            "peak": peak[0] / 1e3, "unit": "TFLOP/s", "frac": achieved / (peak[0] / 1e3),
+            "traffic": traffic,
+            "peak_source": "FP32 FMA throughput measured by bh_probe_fma_peak in this run "
+                           "(MEASURED_PEAKS.json has no FP32 figure; its HBM copy peak is not the bound)",
+            "algorithmic_flops_per_launch": alg_flops, "executed_flops_per_launch": exe_flops,
+            "reference_interactions_per_target": {"body_body": float(mean_pp),
+                                                  "body_cell": float(mean_pc)},
+            "executed_interactions_per_target": {"body_body": float(st[0]) / n,
+                                                 "body_cell": float(st[1]) / n},
+            "walk_ms": t_w * 1e3, "fp64_peak_tflops": peak[1] / 1e3}
 
+        # ---- end to end from pinned host buffers ----
+        hm = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        hx, hy, hz = (torch.empty_like(hm) for _ in range(3))
+        hout = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
+        for h, d in zip((hm, hx, hy, hz), systems[0]):
+            h.copy_(d.cpu())
         L = _lib.lib()
 
         def e2e_call():
-            _lib.check(L.bh_compute_forces_ex(hm.data_ptr(), hx.data_ptr(), hy.data_ptr(), hz.data_ptr(), n,
-                                              C.byref(p), hout.data_ptr(), stream.cuda_stream))
+            _lib.check(L.bh_compute_forces_ex(hm.data_ptr(), hx.data_ptr(), hy.data_ptr(),
+                                              hz.data_ptr(), n, C.byref(p), hout.data_ptr(),
+                                              stream.cuda_stream))
 
-        for _ in range(args.warmup):
+        for _ in range(W):
             e2e_call()
         te = []
-        for _ in range(args.steps):
+        for _ in range(K):
             flush.zero_()
             torch.cuda.synchronize()
             a = torch.cuda.Event(enable_timing=True)
@@ -288,21 +392,150 @@ def run_ours(args):
             b.record(stream)
             b.synchronize()
             te.append(a.elapsed_time(b))
-        e2e_ms = statistics.mean(te)
-        if world > 1:
-            tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
-        line["e2e"] = {"value": world * n / (e2e_ms * 1e-3), "unit": "forces/s",
-                       "ms_per_step": e2e_ms, "h2d_bytes_per_step": 4 * 8 * n,
-                       "d2h_bytes_per_step": 3 * 8 * n, "api": "bh_compute_forces_ex (host arrays)"}
+        plain_e2e_ms = dist_max(statistics.mean(te), dev, world)
+        host_sys = []
+        for i in range(K + W):
+            mm, xx, yy, zz = systems[i]
+            host_sys.append((mm.cpu().numpy(), torch.stack([xx, yy, zz], 1).cpu().numpy()))
+        # the client's inputs and result buffers are pinned ahead of time, as the
+        # plain call's are
+        hreqs = [serving.Server.prepare(serving.Request("force", *host_sys[i])) for i in range(K)]
+        hwarm = [serving.Server.prepare(serving.Request("force", *host_sys[K + i]))
+                 for i in range(W)]
+        served_e2e_total, hmet = serve(hreqs, hwarm)
+        served_e2e_ms = dist_max(served_e2e_total, dev, world) / K
+        same_host = bool(np.array_equal(hreqs[-1].forces, f_plain_last.view(3, n).T.cpu().numpy()))
+        line["e2e"] = {"value": world * n / (served_e2e_ms * 1e-3), "unit": "forces/s",
+                       "ms_per_step": served_e2e_ms, "h2d_bytes_per_step": 4 * 8 * n,
+                       "d2h_bytes_per_step": 3 * 8 * n,
+                       "api": "serving.Server with host requests (pinned in, results copied out)",
+                       "p50_ms": hmet["p50_ms"], "p99_ms": hmet["p99_ms"],
+                       "equal_to_plain_bitwise": same_host,
+                       "plain": {"value": world * n / (plain_e2e_ms * 1e-3), "ms_per_step": plain_e2e_ms,
+                                 "api": "bh_compute_forces_ex (host arrays, the api3d drop-in)"}}
+        del systems, host_sys, hreqs, hwarm, reqs
+
+        # ---- 512 independent systems: batched vs plain loop ----
+        line["batched"] = bench_batch(args, p, dev, local, world, rank)
+
         if rank == 0 and world == 1:
-            line["cpu_baseline"] = cpu_baseline(n, m, q, args.order, samples=32768)
+            m0, q0 = workload(n, seed=1000)
+            line["cpu_baseline"] = cpu_baseline(n, m0, q0, args.order, samples=32768)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batch_workload(count, seed):
+    """``count`` systems, N log-uniform in [1024, 65536], alternating Plummer
+    (b = 1) and uniform-density unit spheres, drawn on the device."""
+    import torch
+
+    from hierarquicos_b200.initial_values import generate_initial_values_device
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(math.log(1024), math.log(65536), count)).astype(np.int64)
+    ms, xs, ys, zs = [], [], [], []
+    for k, nk in enumerate(sizes):
+        prof = "plummer" if k % 2 == 0 else "homogeneous"
+        m, q, _ = generate_initial_values_device(int(nk), -1.0, -1.0, True, False, prof, (1.0, 1.0),
+                                                 seed=seed * 100000 + k, velocities=False)
+        ms.append(m)
+        xs.append(q[0])
+        ys.append(q[1])
+        zs.append(q[2])
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    return sizes, off, (torch.cat(ms), torch.cat(xs), torch.cat(ys), torch.cat(zs))
+
+
+def bench_batch(args, p, dev, local, world, rank):
+    import torch
+
+    from hierarquicos_b200 import autotune
+    from hierarquicos_b200.system import BHSystem, direct_targets
+
+    stream = torch.cuda.current_stream()
+    sizes, off, (m, x, y, z) = batch_workload(args.batch_systems, 77 + rank)
+    ntot = int(off[-1])
+    pt, rep = autotune.tune(m, x, y, z, off, p, reps=2, use_cache=False)
+    out = torch.empty(3 * ntot, dtype=torch.float64, device=dev)
+    sysm = BHSystem(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.mean(ts)
+
+    # plain loop: one call per system, default parameters
+    plain = BHSystem(local)
+    views = [(m[a:b], x[a:b], y[a:b], z[a:b], out[3 * a:3 * b])
+             for a, b in zip(off[:-1].tolist(), off[1:].tolist())]
+
+    def loop():
+        for mm, xx, yy, zz, oo in views:
+            plain.forces(mm, xx, yy, zz, p, out=oo)
+
+    loop()
+    loop_ms = dist_max(timed(loop, 2), dev, world)
+    f_loop = out.clone()
+
+    def batched(pp):
+        return lambda: sysm.forces_batch(m, x, y, z, off, pp, out=out)
+
+    batched(p)()
+    b_default_ms = dist_max(timed(batched(p), max(3, args.steps)), dev, world)
+    same = bool(torch.equal(out, f_loop))
+    batched(pt)()
+    b_ms = dist_max(timed(batched(pt), max(3, args.steps)), dev, world)
+    # CUDA graph of the tuned build + walk (status read after each replay)
+    sysm.build_batch(m, x, y, z, off, pt)
+    sysm.sync()
+    sysm.capture(pt, out)
+
+    def replay():
+        sysm.replay()
+        sysm.sync()
+
+    replay()
+    g_ms = dist_max(timed(replay, max(3, args.steps)), dev, world)
+    # accuracy of the tuned batch on sampled targets of sampled systems
+    rng = np.random.default_rng(5)
+    errs = []
+    f = out.view(-1)
+    for s in rng.choice(len(sizes), 8, replace=False):
+        a, b = int(off[s]), int(off[s + 1])
+        nb = b - a
+        tg = np.sort(rng.choice(nb, min(1024, nb), replace=False))
+        tgt = torch.as_tensor(tg, device=dev)
+        fd = direct_targets(m[a:b], x[a:b], y[a:b], z[a:b], tgt, p.G, p.eps).T
+        fb = torch.stack([f[3 * a + tgt], f[3 * a + nb + tgt], f[3 * a + 2 * nb + tgt]], 1)
+        d = torch.linalg.norm(fb - fd, dim=1) / torch.linalg.norm(fd, dim=1)
+        errs.append(d.cpu().numpy())
+    e = np.concatenate(errs)
+    total = world * ntot
+    return {"workload": f"{len(sizes)} systems, N log-uniform [1024, 65536] (total {ntot}), "
+                        "Plummer b=1 / uniform sphere R=1 alternating, theta 0.5 quadrupole",
+            "plain_loop": {"value": total / (loop_ms * 1e-3), "ms": loop_ms},
+            "batched_default": {"value": total / (b_default_ms * 1e-3), "ms": b_default_ms,
+                                "equal_to_plain_loop_bitwise": same},
+            "batched_tuned": {"value": total / (b_ms * 1e-3), "ms": b_ms,
+                              "params": {"group_size": pt.group_size, "group_span": pt.group_span,
+                                         "leaf_cap": pt.leaf_cap}},
+            "graph_replay": {"value": total / (g_ms * 1e-3), "ms": g_ms},
+            "speedup_over_plain_loop": loop_ms / min(b_ms, g_ms),
+            "rms_rel": float(np.sqrt(np.mean(e * e))), "max_rel": float(e.max()),
+            "unit": "forces/s"}
 
 
 def cpu_baseline(n, m, q, order, samples):
@@ -349,12 +582,13 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * n / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Hernquist ICs)",
-            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded", "theta": THETA,
-                       "eps": EPS, "order": args.order},
+            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, force requests",
+                       "n_per_request": n, "theta": THETA, "eps": EPS, "order": args.order},
             "cpu_baseline": {"value": value, "unit": "forces/s", "cores": vals[0]["cores"],
                              "kind": "port",
-                             "sample": f"per step: full tree build + walk of {samples} seeded targets, scaled to N "
-                                       "(the Fortran reference cannot be compiled here: no Fortran compiler)"},
+                             "sample": f"per step: full tree build + walk of {samples} seeded targets, "
+                                       "scaled to N (the Fortran reference cannot be compiled here: "
+                                       "no Fortran compiler)"},
             "e2e": {"value": value, "unit": "forces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

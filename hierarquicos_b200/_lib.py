@@ -37,7 +37,7 @@ EXPORTED = [
     "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
     "bh_system_build_batch", "bh_system_forces_batch", "bh_system_batch_info",
     "bh_system_capture", "bh_system_replay", "bh_kick_drift", "bh_diagnostics",
-    "bh_kick_drift_systems", "bh_generate_ics",
+    "bh_kick_drift_systems", "bh_generate_ics", "bh_system_reserve",
 ]
 
 BH_NOALLOC_MAX_N = 8192
@@ -115,6 +115,7 @@ def lib():
             "bh_kick_drift": [_vp] * 8 + [_vp, _i, _i64, _d, _d, _d, _vp],
             "bh_diagnostics": [_vp] * 7 + [_vp, _i, _i64, _d, _d, _vp, _vp, _vp],
             "bh_kick_drift_systems": [_vp] * 8 + [_vp, _i, _i64, _vp, _vp],
+            "bh_system_reserve": [_vp, _i64, _i],
             "bh_generate_ics": [_i, _i64, _d, _d, _i, _i, _d, _d, C.c_uint64, _i, _vp, _vp, _vp,
                                 _vp, _vp],
         }

@@ -33,6 +33,12 @@ struct bh_system {
   double *walk_out = nullptr;
   // captured build + walk of the current layout
   cudaGraphExec_t graph = nullptr;
+  // pinned staging of the layout's reduction items; the event marks the end
+  // of the last layout upload, after which ss_host and items_pin may be reused
+  bh::RedItem *items_pin = nullptr;
+  int items_pin_cap = 0;
+  cudaEvent_t layout_ev = nullptr;
+  bool layout_pending = false;
 };
 
 namespace {
@@ -127,6 +133,8 @@ int ensure_capacity(bh_system *s, int64_t n, int nsys, int n_items) {
     b.wstack_cap = s->stack_cap;
   }
   if (!sys_ok) {
+    if (s->layout_pending) cudaEventSynchronize(s->layout_ev);
+    s->layout_pending = false;
     if (b.ss) cudaFree(b.ss);
     if (b.ss_host) cudaFreeHost(b.ss_host);
     if (b.items) cudaFree(b.items);
@@ -141,6 +149,12 @@ int ensure_capacity(bh_system *s, int64_t n, int nsys, int n_items) {
     BH_CUDA(cudaMallocHost((void **)&b.ss_host, (size_t)sc_ * sizeof(bh::SysScalars)));
     BH_CUDA(dalloc(&b.items, ic));
     BH_CUDA(dalloc(&b.partials, 10 * (int64_t)ic));
+    if (s->layout_pending) cudaEventSynchronize(s->layout_ev);
+    s->layout_pending = false;
+    if (s->items_pin) cudaFreeHost(s->items_pin);
+    s->items_pin = nullptr;
+    BH_CUDA(cudaMallocHost((void **)&s->items_pin, (size_t)ic * sizeof(bh::RedItem)));
+    s->items_pin_cap = ic;
     b.sys_cap = sc_;
     b.items_cap = ic;
     b.nsys = 0;
@@ -197,11 +211,18 @@ int set_layout(bh_system *s, const int64_t *off, int nsys, cudaStream_t st) {
       memcmp(s->offsets.data(), off, (size_t)(nsys + 1) * sizeof(int64_t)) == 0)
     return BH_OK;
   drop_graph(s);
-  s->items_host.clear();
+  // pinned staging (pageable host memory for caller-provided workspaces)
+  bh::RedItem *items = s->items_pin;
+  if (s->fixed_buffers || !items) {
+    s->items_host.resize((size_t)count_items(off, nsys));
+    items = s->items_host.data();
+  } else if (s->layout_pending) {
+    BH_CUDA(cudaEventSynchronize(s->layout_ev));  // the previous upload has left the staging
+  }
+  int k = 0;
   for (int q = 0; q < nsys; ++q)
     for (int64_t a = off[q]; a < off[q + 1]; a += bh::kRedChunk)
-      s->items_host.push_back(
-          bh::RedItem{q, 0, a, a + bh::kRedChunk < off[q + 1] ? a + bh::kRedChunk : off[q + 1]});
+      items[k++] = bh::RedItem{q, 0, a, a + bh::kRedChunk < off[q + 1] ? a + bh::kRedChunk : off[q + 1]};
   for (int q = 0; q < nsys; ++q) {
     memset(&b.ss_host[q], 0, sizeof(bh::SysScalars));
     b.ss_host[q].off = off[q];
@@ -210,13 +231,17 @@ int set_layout(bh_system *s, const int64_t *off, int nsys, cudaStream_t st) {
   }
   BH_CUDA(cudaMemcpyAsync(b.ss, b.ss_host, (size_t)nsys * sizeof(bh::SysScalars),
                           cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.items, s->items_host.data(),
-                          s->items_host.size() * sizeof(bh::RedItem), cudaMemcpyHostToDevice, st));
-  b.n_items = (int)s->items_host.size();
+  BH_CUDA(cudaMemcpyAsync(b.items, items, (size_t)k * sizeof(bh::RedItem), cudaMemcpyHostToDevice, st));
+  b.n_items = k;
   b.nsys = nsys;
   bh::launch_layout(b, st);
-  // the host staging areas are reused by the next layout
-  BH_CUDA(cudaStreamSynchronize(st));
+  if (items == s->items_pin) {
+    if (!s->layout_ev) BH_CUDA(cudaEventCreateWithFlags(&s->layout_ev, cudaEventDisableTiming));
+    BH_CUDA(cudaEventRecord(s->layout_ev, st));
+    s->layout_pending = true;
+  } else {
+    BH_CUDA(cudaStreamSynchronize(st));  // pageable staging is reused by the next layout
+  }
   s->offsets.assign(off, off + nsys + 1);
   return BH_OK;
 }
@@ -488,8 +513,20 @@ int bh_system_destroy(bh_system *s) {
   cudaDeviceSynchronize();
   drop_graph(s);
   if (!s->fixed_buffers) free_buffers(s->b);
+  if (s->items_pin) cudaFreeHost(s->items_pin);
+  if (s->layout_ev) cudaEventDestroy(s->layout_ev);
   delete s;
   return BH_OK;
+}
+
+int bh_system_reserve(bh_system *s, int64_t n, int nsys) {
+  if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
+  if (n < 1 || n > (int64_t)(1 << 30) || nsys < 1 || nsys > n)
+    return set_err(BH_ERR_INVALID, "reserve: need 1 <= nsys <= n <= 2^30");
+  BH_CUDA(cudaSetDevice(s->device));
+  // every system adds at most one partial reduction chunk
+  const int64_t items = (n + bh::kRedChunk - 1) / bh::kRedChunk + nsys;
+  return ensure_capacity(s, n, nsys, (int)items);
 }
 
 int bh_system_build(bh_system *s, const double *d_m, const double *d_x, const double *d_y,

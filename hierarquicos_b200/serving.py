@@ -74,7 +74,10 @@ class Request:
     def __post_init__(self):
         if self.kind not in ("force", "leapfrog"):
             raise ValueError("kind must be 'force' or 'leapfrog'")
-        self.n = int(np.asarray(self.m).size)
+        # device-resident request: CUDA tensors in (m (n,), q and p (3, n)),
+        # results stay on the device
+        self.on_device = isinstance(self.m, torch.Tensor) and self.m.is_cuda
+        self.n = int(self.m.numel() if self.on_device else np.asarray(self.m).size)
         if self.kind == "leapfrog" and (self.steps < 1 or self.p is None):
             raise ValueError("a leapfrog request needs momenta and steps >= 1")
         self._done = threading.Event()
@@ -101,7 +104,8 @@ class _Lane:
             self.stream = torch.cuda.Stream(dev)
             self.h2d = torch.cuda.Stream(dev)
             self.d2h = torch.cuda.Stream(dev)
-        self.sys = BHSystem(dev.index)
+        # the lane's workspace, allocated once for its largest tick
+        self.sys = BHSystem(dev.index).reserve(server.max_tick_bodies, server.max_tick_systems)
         self.active: list[Request] = []
         self.state: dict[int, dict] = {}
         self.done_q: collections.deque = collections.deque()
@@ -116,6 +120,9 @@ class _Lane:
     def _stage(self, r: Request):
         dev = self.server.device
         host = r._pinned
+        if r.on_device:
+            self.state[r.id] = host
+            return
         with torch.cuda.stream(self.h2d):
             d = {k: v.to(dev, non_blocking=True) for k, v in host.items()}
             ev = torch.cuda.Event()
@@ -165,6 +172,20 @@ class _Lane:
                 finished.append((r, a, b))
             else:
                 keep.append(r)
+        dev_done = [(r, a, b) for r, a, b in finished if r.on_device]
+        finished = [(r, a, b) for r, a, b in finished if not r.on_device]
+        if dev_done:
+            with torch.cuda.stream(self.stream):
+                for r, a, b in dev_done:
+                    if r.kind == "force":
+                        r._dev_out = {"f": out[3 * a:3 * b].view(3, b - a)}
+                    else:
+                        r._dev_out = {k: cat[k][a:b] for k in ("x", "y", "z", "px", "py", "pz")}
+                    done = torch.cuda.Event()
+                    done.record(self.stream)
+                    with self.done_cv:
+                        self.done_q.append((r, done))
+                        self.done_cv.notify()
         if finished:
             self.d2h.wait_event(ev)
             with torch.cuda.stream(self.d2h):
@@ -229,6 +250,16 @@ class _Lane:
             r, ev = item
             ev.synchronize()
             r.t_done = time.perf_counter()
+            if r.on_device:
+                do = r._dev_out
+                if r.kind == "force":
+                    r.forces = do["f"].T
+                else:
+                    r.q_out = torch.stack([do["x"], do["y"], do["z"]], dim=1)
+                    r.p_out = torch.stack([do["px"], do["py"], do["pz"]], dim=1)
+                self.server._release(r)
+                r._done.set()
+                continue
             ho = r._host_out
             if r.kind == "force":
                 r.forces = ho["f"].numpy().reshape(3, r.n).T
@@ -248,11 +279,13 @@ class Server:
     workspaces and a tick's latency)."""
 
     def __init__(self, params: BHParams | None = None, device=None, hbm_budget: float = 150e9,
-                 max_tick_bodies: int = 1 << 23, lanes: int = 2, **kw):
+                 max_tick_bodies: int = 1 << 23, lanes: int = 2, max_tick_systems: int = 4096,
+                 **kw):
         self.device = as_device(device)
         self.params = params if params is not None else default_params(**kw)
         self.hbm_budget = float(hbm_budget)
         self.max_tick_bodies = int(max_tick_bodies)
+        self.max_tick_systems = int(min(max_tick_systems, max_tick_bodies))
         self.workspace_bytes = lanes * WORKSPACE_BYTES_PER_BODY * self.max_tick_bodies
         if self.workspace_bytes >= self.hbm_budget:
             raise ValueError("hbm_budget does not cover the lanes' workspaces")
@@ -279,7 +312,7 @@ class Server:
             raise ValueError(f"request of {r.n} bodies exceeds a lane's tick ({self.max_tick_bodies})")
         if self.footprint(r.n) > self.hbm_budget - self.workspace_bytes:
             raise ValueError("request larger than the HBM budget")
-        self._pin(r)
+        self.prepare(r)
         if r.arrival is None:
             r.arrival = time.perf_counter()
         with self._cv:
@@ -289,7 +322,32 @@ class Server:
         return r
 
     @staticmethod
+    def prepare(r: Request) -> Request:
+        """Puts a request's inputs where the server reads them (pinned host
+        buffers for host arrays) and allocates its pinned result buffers.  A
+        client that prepares its requests ahead of time keeps these copies
+        out of the requests' latency; ``submit`` prepares the others."""
+        if getattr(r, "_pinned", None) is not None:
+            return r
+        Server._pin(r)
+        return r
+
+    @staticmethod
     def _pin(r: Request):
+        if r.on_device:
+            q = r.q if r.q.shape[0] == 3 else r.q.T
+            d = {"m": r.m.contiguous(), "x": q[0].contiguous(), "y": q[1].contiguous(),
+                 "z": q[2].contiguous()}
+            if r.kind == "leapfrog":
+                p = r.p if r.p.shape[0] == 3 else r.p.T
+                d.update(px=p[0].clone(), py=p[1].clone(), pz=p[2].clone())
+                d.update(x=d["x"].clone(), y=d["y"].clone(), z=d["z"].clone())
+            else:
+                z = torch.zeros(r.n, dtype=torch.float64, device=r.m.device)
+                d.update(px=z, py=z, pz=z)
+            r._pinned = d
+            return
+
         def pin(a):
             t = torch.empty(len(a), dtype=torch.float64, pin_memory=True)
             t.numpy()[:] = a
@@ -356,11 +414,14 @@ class Server:
         with self._cv:
             room = self.hbm_budget - self.workspace_bytes
             bodies = sum(r.n for r in lane.active)
+            systems = len(lane.active)
             while self._pending:
                 r = self._pending[0]
                 fp = self.footprint(r.n)
-                if self._resident + fp > room or bodies + r.n > self.max_tick_bodies:
+                if (self._resident + fp > room or bodies + r.n > self.max_tick_bodies
+                        or systems + 1 > self.max_tick_systems):
                     break
+                systems += 1
                 self._pending.popleft()
                 self._resident += fp
                 self.max_resident = max(self.max_resident, self._resident)

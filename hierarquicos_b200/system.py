@@ -96,6 +96,12 @@ class BHSystem:
                                      C.byref(p), _dptr(out), _stream()))
         return out
 
+    def reserve(self, n: int, nsys: int = 1) -> "BHSystem":
+        """Allocates the workspace for batches of up to n bodies in up to nsys
+        systems, so that builds within those bounds allocate nothing."""
+        check(lib().bh_system_reserve(self._h, int(n), int(nsys)))
+        return self
+
     # -- batches of independent systems --
     def build_batch(self, m, x, y, z, offsets, params: BHParams | None = None,
                     **kw) -> "BHSystem":

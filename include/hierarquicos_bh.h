@@ -142,6 +142,10 @@ int bh_system_forces_batch(bh_system *sys, const double *d_m, const double *d_x,
                            const double *d_y, const double *d_z, const int64_t *offsets,
                            int nsys, const bh_params *p, double *d_out, void *stream);
 
+/* Allocates the workspace for batches of up to n bodies in up to nsys
+ * systems now, so that later builds within those bounds allocate nothing. */
+int bh_system_reserve(bh_system *sys, int64_t n, int nsys);
+
 /* Root node, centre of mass + mass (com4, 4 per system) and root cube side of
  * every system of the last build, copied to HOST arrays (any may be NULL). */
 int bh_system_batch_info(bh_system *sys, int32_t *roots, double *com4, double *ssa);
