@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--bodies", type=int, default=N_DEFAULT, dest="n")
     ap.add_argument("--order", type=int, default=ORDER)
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--group-size", type=int, default=64)
@@ -549,6 +549,7 @@ def cpu_baseline(n, m, q, order, samples):
     tree = oracle.MortonTree(m, x, y, z, L=21, ssa=1.2, use_quadrupole=order >= 4, fma_mode=1)
     t_build = time.perf_counter() - t0
     rng = np.random.default_rng(7)
+    samples = min(samples, n)
     tg = rng.choice(n, samples, replace=False)
     t0 = time.perf_counter()
     tree.forces_targets(tg, 1.0, EPS * EPS, THETA * THETA, order >= 4)

@@ -1,0 +1,73 @@
+"""Multi-process logic of the benchmark on the CPU (gloo, world size 2): the
+max-over-ranks timing reduction, and the reference arm under torchrun (rank 0
+alone runs and prints one line; the other ranks exit without work)."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, ROOT)
+    import bench
+
+    got = bench.dist_max(10.0 + rank, torch.device("cpu"), world)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, got))
+
+
+def _free_port():
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_timings_reduce_to_the_max_over_ranks():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res == {0: 11.0, 1: 11.0}
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
+           "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--bodies", "4096"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+@pytest.mark.parametrize("rank", ["1"])
+def test_reference_arm_other_ranks_exit_without_work(rank):
+    env = dict(os.environ, RANK=rank, WORLD_SIZE="2", LOCAL_RANK=rank)
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--bodies", "4096"], cwd=ROOT,
+                       env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == ""
