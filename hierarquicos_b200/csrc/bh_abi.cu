@@ -265,6 +265,7 @@ int check_params(const bh_params *p, int64_t n) {
   if (p->strict_keys < 0 || p->strict_keys > 2) return set_err(BH_ERR_INVALID, "strict_keys must be 0, 1 or 2");
   if (p->group_span != 0 && (p->group_span < p->group_size || p->group_span > (1 << 20)))
     return set_err(BH_ERR_INVALID, "group_span must be 0 or in [group_size, 2^20]");
+  if (p->mac != 0 && p->mac != 1) return set_err(BH_ERR_INVALID, "mac must be 0 or 1");
   return BH_OK;
 }
 
@@ -320,6 +321,7 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
   w.group_size = p->group_size;
   w.leaf_cap = p->leaf_cap;
   w.count_stats = p->count_stats;
+  w.mac = p->mac;
   return w;
 }
 

@@ -68,6 +68,21 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(T *sink, T a, T b) {
   if (s == (T)12345.678) sink[threadIdx.x] = s;  // keeps the chains alive
 }
 
+// The same chains with paired FP32 instructions (two FMAs per instruction).
+__global__ void __launch_bounds__(256) fma2_probe_kernel(float *sink, float a, float b) {
+  const float2 av = make_float2(a, a), bv = make_float2(b, b);
+  const float f = (float)threadIdx.x;
+  float2 v0 = make_float2(f, f + 1), v1 = make_float2(f + 2, f + 3), v2 = make_float2(f + 4, f + 5),
+         v3 = make_float2(f + 6, f + 7);
+#pragma unroll 16
+  for (int i = 0; i < kProbeIters; ++i) {
+    v0 = __ffma2_rn(v0, av, bv); v1 = __ffma2_rn(v1, av, bv);
+    v2 = __ffma2_rn(v2, av, bv); v3 = __ffma2_rn(v3, av, bv);
+  }
+  const float s = v0.x + v0.y + v1.x + v1.y + v2.x + v2.y + v3.x + v3.y;
+  if (s == 12345.678f) sink[threadIdx.x] = s;
+}
+
 }  // namespace
 
 void launch_direct(const double *m, const double *x, const double *y, const double *z, int64_t n,
@@ -78,7 +93,8 @@ void launch_direct(const double *m, const double *x, const double *y, const doub
   direct_kernel<<<grid, kDirThreads, 0, s>>>(m, x, y, z, n, targets, nt, G, eps2, out_kind, out);
 }
 
-// GFLOP/s of FP32 and FP64 FMA (2 flops each) on independent chains.
+// GFLOP/s of FMA (2 flops each) on independent chains: [0] FP32, [1] FP64,
+// [2] FP32 issued as paired (f32x2) instructions.
 int probe_fma(double *gflops2) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -92,12 +108,13 @@ int probe_fma(double *gflops2) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const double flops = 2.0 * 8.0 * kProbeIters * (double)blocks * threads;
-  for (int which = 0; which < 2; ++which) {
+  for (int which = 0; which < 3; ++which) {
     float best = 1e30f;
     for (int rep = 0; rep < 5; ++rep) {
       cudaEventRecord(e0);
       if (which == 0) fma_probe_kernel<float><<<blocks, threads>>>(fs, 0.999f, 1e-3f);
-      else fma_probe_kernel<double><<<blocks, threads>>>(ds, 0.999, 1e-3);
+      else if (which == 1) fma_probe_kernel<double><<<blocks, threads>>>(ds, 0.999, 1e-3);
+      else fma2_probe_kernel<<<blocks, threads>>>(fs, 0.999f, 1e-3f);
       cudaEventRecord(e1);
       cudaEventSynchronize(e1);
       float ms = 0.f;

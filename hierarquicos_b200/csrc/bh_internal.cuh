@@ -175,6 +175,7 @@ struct WalkParams {
   int group_size;  // 32 or 64
   int leaf_cap;
   int count_stats;
+  int mac;         // 0 box distance, 1 box distance or every member's own MAC
 };
 // Returns the number of warp slots used (for stack sizing).
 void launch_walk(int64_t n, const WalkParams &p, Buffers &b, double *out, cudaStream_t s);

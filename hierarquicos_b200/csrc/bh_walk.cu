@@ -34,6 +34,11 @@ namespace bh {
 namespace {
 
 constexpr int kWalkWarps = 4;
+// resident blocks per SM the FP32 walk is compiled for (register budget)
+#ifndef BH_WALK_MIN_BLOCKS
+#define BH_WALK_MIN_BLOCKS 4
+#endif
+template <typename T> constexpr int walk_min_blocks() { return sizeof(T) == 4 ? BH_WALK_MIN_BLOCKS : 1; }
 constexpr int kCellQ = 64;
 constexpr int kBodyPerLane = 16;
 constexpr int kBodyQ = 32 + kWarp * kBodyPerLane;  // 544
@@ -90,7 +95,7 @@ struct WalkArgs {
   double *out;
   int64_t n;
   double theta2, G, eps2;
-  int out_kind, leaf_cap, count_stats;
+  int out_kind, leaf_cap, count_stats, mac;
 };
 
 template <typename T>
@@ -126,42 +131,46 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int &total) {
 //   [12..23] O1..O10, O12, O13     (octupole only)
 // The factors 7.5 and -1.5 of the reference's cell formula
 // (octree_default.f90:2024-2027) are folded in here once per staged cell.
-template <typename T, int ORDER>
+// Word k goes to w[k * STR]: STR = 1 for the FP64 walk, 2 for the paired FP32
+// walk, whose stage holds cells 2i and 2i+1 interleaved word by word.
+template <typename T, int ORDER, int STR = 1>
 __device__ __forceinline__ void stage_cell(T *w, int j, const WalkArgs &a, const double gc[3],
                                            double inv_s, double inv_m, double nq, double no) {
   const double4 c = a.com[j];
-  w[0] = (T)((c.x - gc[0]) * inv_s);
-  w[1] = (T)((c.y - gc[1]) * inv_s);
-  w[2] = (T)((c.z - gc[2]) * inv_s);
-  w[3] = (T)(c.w * inv_m);
+  w[0 * STR] = (T)((c.x - gc[0]) * inv_s);
+  w[1 * STR] = (T)((c.y - gc[1]) * inv_s);
+  w[2 * STR] = (T)((c.z - gc[2]) * inv_s);
+  w[3 * STR] = (T)(c.w * inv_m);
   if (ORDER >= 4) {
     if (sizeof(T) == 4) {
       const float4 q0 = a.fq[2 * (int64_t)j], q1 = a.fq[2 * (int64_t)j + 1];
-      w[4] = (T)(7.5f * q0.x); w[5] = (T)(7.5f * q0.y); w[6] = (T)(7.5f * q0.z); w[7] = (T)(7.5f * q0.w);
-      w[8] = (T)(7.5f * q1.x); w[9] = (T)(7.5f * q1.y); w[10] = (T)(-1.5f * q1.z);
+      w[4 * STR] = (T)(7.5f * q0.x); w[5 * STR] = (T)(7.5f * q0.y); w[6 * STR] = (T)(7.5f * q0.z);
+      w[7 * STR] = (T)(7.5f * q0.w); w[8 * STR] = (T)(7.5f * q1.x); w[9 * STR] = (T)(7.5f * q1.y);
+      w[10 * STR] = (T)(-1.5f * q1.z);
     } else {
       const double *q = a.quad + 6 * (int64_t)j;
       const double q0 = q[0] * nq, q1 = q[1] * nq, q2 = q[2] * nq;
-      w[4] = (T)(7.5 * q0); w[5] = (T)(7.5 * q1); w[6] = (T)(7.5 * q2);
-      w[7] = (T)(7.5 * q[3] * nq); w[8] = (T)(7.5 * q[4] * nq); w[9] = (T)(7.5 * q[5] * nq);
-      w[10] = (T)(-1.5 * (q0 + q1 + q2));
+      w[4 * STR] = (T)(7.5 * q0); w[5 * STR] = (T)(7.5 * q1); w[6 * STR] = (T)(7.5 * q2);
+      w[7 * STR] = (T)(7.5 * q[3] * nq); w[8 * STR] = (T)(7.5 * q[4] * nq);
+      w[9 * STR] = (T)(7.5 * q[5] * nq);
+      w[10 * STR] = (T)(-1.5 * (q0 + q1 + q2));
     }
-    w[11] = (T)0;
+    w[11 * STR] = (T)0;
   }
   if (ORDER >= 8) {
     if (sizeof(T) == 4) {
       const float4 *f = a.fo + 4 * (int64_t)j;
       const float4 o0 = f[0], o1 = f[1], o2 = f[2], o3 = f[3];
-      w[12] = (T)o0.x; w[13] = (T)o0.y; w[14] = (T)o0.z; w[15] = (T)o0.w;
-      w[16] = (T)o1.x; w[17] = (T)o1.y; w[18] = (T)o1.z; w[19] = (T)o1.w;
-      w[20] = (T)o2.x; w[21] = (T)o2.y; w[22] = (T)o2.z; w[23] = (T)o2.w;
-      w[11] = (T)o3.x;
+      w[12 * STR] = (T)o0.x; w[13 * STR] = (T)o0.y; w[14 * STR] = (T)o0.z; w[15 * STR] = (T)o0.w;
+      w[16 * STR] = (T)o1.x; w[17 * STR] = (T)o1.y; w[18 * STR] = (T)o1.z; w[19 * STR] = (T)o1.w;
+      w[20 * STR] = (T)o2.x; w[21 * STR] = (T)o2.y; w[22 * STR] = (T)o2.z; w[23 * STR] = (T)o2.w;
+      w[11 * STR] = (T)o3.x;
     } else {
       const double *o = a.oct + 14 * (int64_t)j;
-      for (int k = 0; k < 10; ++k) w[12 + k] = (T)(o[k] * no);
-      w[22] = (T)(o[11] * no);
-      w[23] = (T)(o[12] * no);
-      w[11] = (T)(o[13] * no);
+      for (int k = 0; k < 10; ++k) w[(12 + k) * STR] = (T)(o[k] * no);
+      w[22 * STR] = (T)(o[11] * no);
+      w[23 * STR] = (T)(o[12] * no);
+      w[11 * STR] = (T)(o[13] * no);
     }
   }
 }
@@ -267,6 +276,91 @@ __device__ __forceinline__ void cell_force(const T *w, T rx, T ry, T rz, T eps2,
   bz = fma(sA, dz, fma(t, qz, fma(r3i, oz, bz)));
 }
 
+// ---- paired FP32 (sm_100 f32x2 instructions) ----
+//
+// The FP32 walk evaluates two staged entries (cells j and j+1, or bodies) per
+// instruction: every operand is a float2 whose halves belong to the two
+// entries, and the target's coordinates are the same in both halves.  Each half
+// is rounded exactly like the scalar operation it replaces.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 rsqrt2(float2 x) { return make_float2(fast_rsqrt(x.x), fast_rsqrt(x.y)); }
+
+// Two body-body terms; (nrx, nry, nrz) is minus the target's position.
+template <bool SOFT>
+__device__ __forceinline__ void body_force2(float2 sx, float2 sy, float2 sz, float2 sm, float2 nrx,
+                                            float2 nry, float2 nrz, float2 eps2, float2 &bx,
+                                            float2 &by, float2 &bz) {
+  const float2 dx = add2(sx, nrx), dy = add2(sy, nry), dz = add2(sz, nrz);
+  float2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, eps2)));
+  if (!SOFT) { r2.x = fmaxf(r2.x, r2_floor<float>()); r2.y = fmaxf(r2.y, r2_floor<float>()); }
+  const float2 ri = rsqrt2(r2);
+  const float2 f = mul2(mul2(sm, ri), mul2(ri, ri));
+  bx = fma2(f, dx, bx); by = fma2(f, dy, by); bz = fma2(f, dz, bz);
+}
+
+// Two cell terms, the formula of cell_force; w[k] holds word k of both cells.
+template <int ORDER>
+__device__ __forceinline__ void cell_force2(const float2 *w, float2 nrx, float2 nry, float2 nrz,
+                                            float2 eps2, float2 &bx, float2 &by, float2 &bz) {
+  const float2 dx = add2(w[0], nrx), dy = add2(w[1], nry), dz = add2(w[2], nrz);
+  const float2 r2 = fma2(dx, dx, fma2(dy, dy, fma2(dz, dz, eps2)));
+  const float2 rinv = rsqrt2(r2);
+  const float2 r2i = mul2(rinv, rinv);
+  const float2 r3i = mul2(rinv, r2i);
+  if (ORDER < 4) {
+    const float2 f = mul2(w[3], r3i);
+    bx = fma2(f, dx, bx); by = fma2(f, dy, by); bz = fma2(f, dz, bz);
+    return;
+  }
+  const float2 qx = fma2(w[4], dx, fma2(w[7], dy, mul2(w[8], dz)));
+  const float2 qy = fma2(w[7], dx, fma2(w[5], dy, mul2(w[9], dz)));
+  const float2 qz = fma2(w[8], dx, fma2(w[9], dy, mul2(w[6], dz)));
+  const float2 dqd = fma2(dx, qx, fma2(dy, qy, mul2(dz, qz)));
+  const float2 A = fma2(dqd, mul2(r2i, r2i), fma2(w[10], r2i, w[3]));
+  const float2 sA = mul2(r3i, A);
+  const float2 t = mul2(splat(-0.4f), mul2(r3i, r2i));
+  if (ORDER < 8) {
+    bx = fma2(sA, dx, fma2(t, qx, bx));
+    by = fma2(sA, dy, fma2(t, qy, by));
+    bz = fma2(sA, dz, fma2(t, qz, bz));
+    return;
+  }
+  const float2 O1 = w[12], O2 = w[13], O3 = w[14], O4 = w[15], O5 = w[16], O6 = w[17], O7 = w[18],
+               O8 = w[19], O9 = w[20], O10 = w[21], O12 = w[22], O13 = w[23], O14 = w[11];
+  const float2 r4i = mul2(r2i, r2i);
+  const float2 s7 = mul2(splat(7.5f), r4i);
+  const float2 s5 = mul2(splat(-1.5f), r2i);
+  const float2 s9 = mul2(mul2(splat(-17.5f), r4i), r2i);
+  const float2 xx = mul2(dx, dx), yy = mul2(dy, dy), zz = mul2(dz, dz), xy = mul2(dx, dy),
+               xz = mul2(dx, dz), yz = mul2(dy, dz);
+  const float2 two = splat(2.0f), three = splat(3.0f);
+  const float2 oc = mul2(s7, fma2(dx, O12, fma2(dy, O13, mul2(dz, O14))));
+  float2 ox = fma2(s5, O12, mul2(dx, oc)), oy = fma2(s5, O13, mul2(dy, oc)),
+         oz = fma2(s5, O14, mul2(dz, oc));
+  ox = fma2(s7, fma2(two, fma2(xy, O4, fma2(xz, O7, mul2(yz, O10))),
+                     fma2(xx, O1, fma2(yy, O2, mul2(zz, O3)))), ox);
+  oy = fma2(s7, fma2(two, fma2(xy, O2, fma2(xz, O10, mul2(yz, O8))),
+                     fma2(xx, O4, fma2(yy, O5, mul2(zz, O6)))), oy);
+  oz = fma2(s7, fma2(two, fma2(xy, O10, fma2(xz, O3, mul2(yz, O6))),
+                     fma2(xx, O7, fma2(yy, O8, mul2(zz, O9)))), oz);
+  float2 c3 = fma2(mul2(xx, dx), O1, fma2(mul2(yy, dy), O5, mul2(mul2(zz, dz), O9)));
+  c3 = fma2(three, fma2(mul2(xx, dy), O4, fma2(mul2(xx, dz), O7, mul2(mul2(xy, dy), O2))), c3);
+  c3 = fma2(three, fma2(mul2(yy, dz), O8, fma2(mul2(xz, dz), O3, mul2(mul2(yz, dz), O6))), c3);
+  c3 = fma2(mul2(splat(6.0f), xy), mul2(dz, O10), c3);
+  c3 = mul2(s9, c3);
+  ox = fma2(dx, c3, ox); oy = fma2(dy, c3, oy); oz = fma2(dz, c3, oz);
+  bx = fma2(sA, dx, fma2(t, qx, fma2(r3i, ox, bx)));
+  by = fma2(sA, dy, fma2(t, qy, fma2(r3i, oy, by)));
+  bz = fma2(sA, dz, fma2(t, qz, fma2(r3i, oz, bz)));
+}
+
+// A staged entry that contributes exactly zero: no mass, no moments, far from
+// every target (positions are in root-cube units, |x| <= ~1).
+constexpr float kPadPos = 1.0e4f;
+
 struct WalkCounters {
   unsigned long long pp = 0, pc = 0, tests = 0;
   int err = 0;
@@ -323,6 +417,15 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
   }
 #pragma unroll
   for (int k = 0; k < 3; ++k) { blo[k] = warp_min(blo[k]); bhi[k] = warp_max(bhi[k]); }
+  // every member lies within `diag` of every point of the box
+  const T diag = sqrt((bhi[0] - blo[0]) * (bhi[0] - blo[0]) + (bhi[1] - blo[1]) * (bhi[1] - blo[1]) +
+                      (bhi[2] - blo[2]) * (bhi[2] - blo[2]));
+  const T inv_theta2 = theta2 > (T)0 ? (T)1 / theta2 : (T)INFINITY;
+  // radius of the members' sphere about the group centre
+  T rad2 = (T)0;
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) rad2 = max(rad2, fma(rx[t], rx[t], fma(ry[t], ry[t], rz[t] * rz[t])));
+  const T rad = sqrt(warp_max(rad2));
 
   auto accumulate = [&](const T (&bx)[TPL], const T (&by)[TPL], const T (&bz)[TPL]) {
 #pragma unroll
@@ -334,48 +437,130 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
       }
     }
   };
+  // FP32: paired evaluation; target coordinates negated and duplicated once
+  constexpr bool kPaired = sizeof(T) == 4;
+  float2 nrx[TPL], nry[TPL], nrz[TPL];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    nrx[t] = splat(-(float)rx[t]); nry[t] = splat(-(float)ry[t]); nrz[t] = splat(-(float)rz[t]);
+  }
+  const float2 eps2p = splat((float)eps2);
   // evaluate the nb queue entries ending at position `end`
   auto eval_bodies = [&](int end, int nb) {
-    if (lane < nb) {
-      const int p = S.bodyq[end - nb + lane];
-      const double4 s = a.spos[p];
-      T *w = S.stage + lane * 4;
-      w[0] = (T)((s.x - gc[0]) * inv_s);
-      w[1] = (T)((s.y - gc[1]) * inv_s);
-      w[2] = (T)((s.z - gc[2]) * inv_s);
-      w[3] = (T)(s.w * inv_m);
-    }
-    __syncwarp();
-    T bx[TPL], by[TPL], bz[TPL];
+    if constexpr (kPaired) {
+      // stage: body pair i at [8i, 8i + 8) as (x, x', y, y', z, z', m, m'); an
+      // odd count is padded with a massless far body
+      float *w = reinterpret_cast<float *>(S.stage) + (lane >> 1) * 8 + (lane & 1);
+      if (lane < nb) {
+        const int p = S.bodyq[end - nb + lane];
+        const double4 s = a.spos[p];
+        w[0] = (float)((s.x - gc[0]) * inv_s);
+        w[2] = (float)((s.y - gc[1]) * inv_s);
+        w[4] = (float)((s.z - gc[2]) * inv_s);
+        w[6] = (float)(s.w * inv_m);
+      } else if (lane == nb && (nb & 1)) {
+        w[0] = w[2] = w[4] = kPadPos;
+        w[6] = 0.0f;
+      }
+      __syncwarp();
+      float2 bx[TPL], by[TPL], bz[TPL];
 #pragma unroll
-    for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = make_float2(0.0f, 0.0f);
+      const int np = (nb + 1) >> 1;
+      const float4 *st = reinterpret_cast<const float4 *>(S.stage);
+      for (int j = 0; j < np; ++j) {
+        const float4 u = st[2 * j], v = st[2 * j + 1];
+        const float2 sx = make_float2(u.x, u.y), sy = make_float2(u.z, u.w);
+        const float2 sz = make_float2(v.x, v.y), sm = make_float2(v.z, v.w);
+#pragma unroll
+        for (int t = 0; t < TPL; ++t)
+          body_force2<SOFT>(sx, sy, sz, sm, nrx[t], nry[t], nrz[t], eps2p, bx[t], by[t], bz[t]);
+      }
+      T sx[TPL], sy[TPL], sz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        sx[t] = bx[t].x + bx[t].y; sy[t] = by[t].x + by[t].y; sz[t] = bz[t].x + bz[t].y;
+      }
+      accumulate(sx, sy, sz);
+    } else {
+      if (lane < nb) {
+        const int p = S.bodyq[end - nb + lane];
+        const double4 s = a.spos[p];
+        T *w = S.stage + lane * 4;
+        w[0] = (T)((s.x - gc[0]) * inv_s);
+        w[1] = (T)((s.y - gc[1]) * inv_s);
+        w[2] = (T)((s.z - gc[2]) * inv_s);
+        w[3] = (T)(s.w * inv_m);
+      }
+      __syncwarp();
+      T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
 #pragma unroll 2
-    for (int j = 0; j < nb; ++j) {
-      T w[4];
-      load_words<4>(S.stage + j * 4, w);
+      for (int j = 0; j < nb; ++j) {
+        T w[4];
+        load_words<4>(S.stage + j * 4, w);
 #pragma unroll
-      for (int t = 0; t < TPL; ++t)
-        body_force<T, SOFT>(w[0], w[1], w[2], w[3], rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+        for (int t = 0; t < TPL; ++t)
+          body_force<T, SOFT>(w[0], w[1], w[2], w[3], rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+      }
+      accumulate(bx, by, bz);
     }
-    accumulate(bx, by, bz);
     wc.pp += (unsigned long long)nb * gn;
     __syncwarp();
   };
   auto eval_cells = [&](int end, int nc) {
-    if (lane < nc)
-      stage_cell<T, ORDER>(S.stage + lane * W, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
-    __syncwarp();
-    T bx[TPL], by[TPL], bz[TPL];
+    if constexpr (kPaired) {
+      // stage: cell pair i at [2Wi, 2W(i + 1)), word k of both cells at 2k, 2k + 1;
+      // an odd count is padded with an empty far cell
+      float *w = reinterpret_cast<float *>(S.stage) + (lane >> 1) * 2 * W + (lane & 1);
+      if (lane < nc) {
+        stage_cell<float, ORDER, 2>(w, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
+      } else if (lane == nc && (nc & 1)) {
 #pragma unroll
-    for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
+        for (int k = 3; k < W; ++k) w[2 * k] = 0.0f;
+        w[0] = w[2] = w[4] = kPadPos;
+      }
+      __syncwarp();
+      float2 bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = make_float2(0.0f, 0.0f);
+      const int np = (nc + 1) >> 1;
+      for (int j = 0; j < np; ++j) {
+        const float4 *st = reinterpret_cast<const float4 *>(S.stage) + j * (W / 2);
+        float2 cw[W];
+#pragma unroll
+        for (int k = 0; k < W / 2; ++k) {
+          const float4 v = st[k];
+          cw[2 * k] = make_float2(v.x, v.y);
+          cw[2 * k + 1] = make_float2(v.z, v.w);
+        }
+#pragma unroll
+        for (int t = 0; t < TPL; ++t)
+          cell_force2<ORDER>(cw, nrx[t], nry[t], nrz[t], eps2p, bx[t], by[t], bz[t]);
+      }
+      T sx[TPL], sy[TPL], sz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        sx[t] = bx[t].x + bx[t].y; sy[t] = by[t].x + by[t].y; sz[t] = bz[t].x + bz[t].y;
+      }
+      accumulate(sx, sy, sz);
+    } else {
+      if (lane < nc)
+        stage_cell<T, ORDER>(S.stage + lane * W, S.cellq[end - nc + lane], a, gc, inv_s, inv_m, nq, no);
+      __syncwarp();
+      T bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = (T)0;
 #pragma unroll 2
-    for (int j = 0; j < nc; ++j) {
-      T w[W];
-      load_words<W>(S.stage + j * W, w);
+      for (int j = 0; j < nc; ++j) {
+        T w[W];
+        load_words<W>(S.stage + j * W, w);
 #pragma unroll
-      for (int t = 0; t < TPL; ++t) cell_force<T, ORDER>(w, rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+        for (int t = 0; t < TPL; ++t) cell_force<T, ORDER>(w, rx[t], ry[t], rz[t], eps2, bx[t], by[t], bz[t]);
+      }
+      accumulate(bx, by, bz);
     }
-    accumulate(bx, by, bz);
     wc.pc += (unsigned long long)nc * gn;
     __syncwarp();
   };
@@ -398,19 +583,51 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
     __syncwarp();
     int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
     int4 mt = make_int4(0, 0, 0, 0);
+    T dx = (T)0, dy = (T)0, dz = (T)0, size2 = (T)0;
+    bool cand = false;
     if (node >= 0) {
       mt = a.meta[node];
       const double4 c = a.com[node];
-      const T dx = (T)((c.x - gc[0]) * inv_s), dy = (T)((c.y - gc[1]) * inv_s),
-              dz = (T)((c.z - gc[2]) * inv_s);
+      dx = (T)((c.x - gc[0]) * inv_s); dy = (T)((c.y - gc[1]) * inv_s); dz = (T)((c.z - gc[2]) * inv_s);
       const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
       const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
       const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
       const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
-      const T size2 = (T)ldexp(1.0, -2 * mt.z);
-      if (size2 <= theta2 * d2) cls = 1;
-      else if (mt.y <= a.leaf_cap || mt.w == 0) cls = 2;
-      else cls = 3;
+      size2 = (T)ldexp(1.0, -2 * mt.z);
+      if (size2 <= theta2 * d2) {
+        cls = 1;
+      } else {
+        cls = (mt.y <= a.leaf_cap || mt.w == 0) ? 2 : 3;
+        if (a.mac == 1 && (mt.x + mt.y <= gf || mt.x >= gf + gn)) {
+          // holds no member: accept when every member passes its own MAC.
+          // Every member is at least |c| - rad from the centre of mass (the
+          // sphere bound); otherwise the members are tested one by one below
+          // if the nearest of them (at most `diag` beyond the box) may pass.
+          const T reach = sqrt(size2 * inv_theta2);
+          const T dc = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+          if (dc - rad >= reach) {
+            cls = 1;
+          } else {
+            const T r2 = reach - diag;
+            cand = r2 <= (T)0 || r2 * r2 <= d2;
+          }
+        }
+      }
+    }
+    // members' own MAC (morton_octree.f90:701-706: size^2 <= theta^2 d^2 with
+    // d from the member to the centre of mass), all members at once
+    for (unsigned pend = __ballot_sync(kFull, cand); pend; pend &= pend - 1) {
+      const int src = __ffs(pend) - 1;
+      const T cx = __shfl_sync(kFull, dx, src), cy = __shfl_sync(kFull, dy, src),
+              cz = __shfl_sync(kFull, dz, src), cs2 = __shfl_sync(kFull, size2, src);
+      T dmin = (T)INFINITY;
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        const T ux = cx - rx[t], uy = cy - ry[t], uz = cz - rz[t];
+        dmin = min(dmin, fma(ux, ux, fma(uy, uy, uz * uz)));
+      }
+      dmin = warp_min(dmin);
+      if (lane == src && cs2 <= theta2 * dmin) cls = 1;
     }
     wc.tests += take;
     group_tests += take;
@@ -500,7 +717,7 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
 // Persistent warps take groups from a global cursor.  With 64-body groups a
 // group of <= 32 bodies runs the one-target-per-lane path.
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
-__global__ void __launch_bounds__(kWalkWarps * kWarp)
+__global__ void __launch_bounds__(kWalkWarps * kWarp, walk_min_blocks<T>())
 group_walk_kernel(WalkArgs a) {
   __shared__ WarpSmem<T, ORDER> shm[kWalkWarps];
   const int lane = threadIdx.x & (kWarp - 1), wid = threadIdx.x / kWarp;
@@ -715,6 +932,7 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   a.stats = b.stats; a.out = out; a.n = n;
   a.theta2 = p.theta2; a.G = p.G; a.eps2 = p.eps2;
   a.out_kind = p.out_kind; a.leaf_cap = p.leaf_cap; a.count_stats = p.count_stats;
+  a.mac = p.mac;
   return a;
 }
 

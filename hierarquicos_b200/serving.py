@@ -112,6 +112,9 @@ class _Lane:
         self.done_cv = threading.Condition()
         self.ticks = 0
         self.tick_bodies = 0
+        # per tick: host seconds spent enqueuing it and CUDA events around its
+        # device work (read by Server.metrics)
+        self.tick_log: collections.deque = collections.deque(maxlen=4096)
         self.thread = threading.Thread(target=self._run, name=f"bh-lane-{index}", daemon=True)
         self.finisher = threading.Thread(target=self._finish_loop, name=f"bh-done-{index}",
                                          daemon=True)
@@ -141,7 +144,10 @@ class _Lane:
         off = np.zeros(len(act) + 1, np.int64)
         off[1:] = np.cumsum(sizes)
         n = int(off[-1])
+        t_host = time.perf_counter()
+        ev_begin = torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(self.stream):
+            ev_begin.record(self.stream)
             st = [self.state[r.id] for r in act]
             cat = {k: torch.cat([s[k] for s in st]) for k in ("m", "x", "y", "z", "px", "py", "pz")}
             out = torch.empty(3 * n, dtype=torch.float64, device=dev)
@@ -161,8 +167,9 @@ class _Lane:
                     _dptr(cat["m"]), _dptr(out), _dptr(cat["x"]), _dptr(cat["y"]),
                     _dptr(cat["z"]), _dptr(cat["px"]), _dptr(cat["py"]), _dptr(cat["pz"]),
                     _dptr(d_off), len(act), n, _dptr(d_coef), self.stream.cuda_stream))
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(self.stream)
+        self.tick_log.append((time.perf_counter() - t_host, ev_begin, ev))
         keep = []
         finished = []
         for i, r in enumerate(act):
@@ -448,10 +455,26 @@ class Server:
         t0 = min(r.arrival for r in rs)
         t1 = max(r.t_done for r in rs)
         forces = sum(r.n * r.evals_needed for r in rs)
+        host_ms, dev_ms, gap_ms = [], [], []
+        for ln in self.lanes:
+            prev = None
+            for h, b, e in ln.tick_log:
+                if not e.query():
+                    continue
+                host_ms.append(h * 1e3)
+                dev_ms.append(b.elapsed_time(e))
+                if prev is not None:
+                    gap_ms.append(prev.elapsed_time(b))  # device idle of the lane between ticks
+                prev = e
+        ticks = {"host_ms_mean": float(np.mean(host_ms)) if host_ms else None,
+                 "device_ms_mean": float(np.mean(dev_ms)) if dev_ms else None,
+                 "device_ms_max": float(np.max(dev_ms)) if dev_ms else None,
+                 "lane_gap_ms_mean": float(np.mean(gap_ms)) if gap_ms else None,
+                 "lane_gap_ms_max": float(np.max(gap_ms)) if gap_ms else None}
         return {"requests": len(rs), "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
                 "wall_s": t1 - t0, "forces": int(forces), "forces_per_s": forces / (t1 - t0),
                 "ticks": sum(ln.ticks for ln in self.lanes),
                 "mean_tick_bodies": sum(ln.tick_bodies for ln in self.lanes)
                 / max(1, sum(ln.ticks for ln in self.lanes)),
-                "max_resident_bytes": self.max_resident}
+                "max_resident_bytes": self.max_resident, "tick_times": ticks}

@@ -61,11 +61,16 @@ typedef struct bh_params {
     int group_span;   /* target groups: consecutive subtrees of <= group_span bodies are
                          concatenated in key order and cut into groups of group_size;
                          0 = 2 * group_size                                         */
-    int reserved[2];
+    int mac;          /* group walk acceptance of a node: 0 the group's box distance
+                         (octree_default.f90:1927-1936); 1 also accept a node that
+                         fails it when it holds none of the group's bodies and passes
+                         every group member's own MAC (morton_octree.f90:701-706)   */
+    int reserved[1];
 } bh_params;
 
 /* Defaults: theta 0.5, G 1, eps 0, order 4, forces, depth 21, FP32, amp 1.2,
- * group 64, leaf_cap 8, com_mode 1, strict_keys 1, count_stats 0, group_span 0. */
+ * group 64, leaf_cap 8, com_mode 1, strict_keys 1, count_stats 0, group_span 0,
+ * mac 0. */
 void bh_params_default(bh_params *p);
 
 const char *bh_version(void);
@@ -248,8 +253,9 @@ int bh_generate_ics(int profile, int64_t n, double size_qs, double size_ps, int 
                     double G, double par, uint64_t seed, int velocities, double *d_m,
                     double *d_q, double *d_p, double *d_scratch, void *stream);
 
-/* FP32 and FP64 fused-multiply-add throughput probe (independent chains,
- * CUDA events): writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64). */
+/* Fused-multiply-add throughput probe (independent chains, CUDA events):
+ * writes GFLOP/s into gflops2[0] (FP32), gflops2[1] (FP64) and gflops2[2]
+ * (FP32 issued as paired f32x2 instructions); gflops2 holds 3 doubles. */
 int bh_probe_fma_peak(int device, double *gflops2);
 
 #ifdef __cplusplus

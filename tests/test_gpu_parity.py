@@ -158,17 +158,21 @@ def test_reference_walk_matches_oracle(bh, oracle_mod, order):
 @pytest.mark.parametrize("order", [1, 4, 8])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("group_size", [32, 64])
-def test_group_walk_accuracy(bh, oracle_mod, order, precision, group_size):
+@pytest.mark.parametrize("mac,theta", [(0, 0.5), (1, 0.5), (1, 0.3), (1, 0.7)])
+def test_group_walk_accuracy(bh, oracle_mod, order, precision, group_size, mac, theta):
     """Group walk vs the FP64 direct sum and vs the reference walk.
 
-    Tolerances: the group walk's RMS relative error against the direct sum is
-    at most 1.05x the reference walk's + 2e-6 (FP32 rounding), and its RMS
-    relative difference from the reference walk's forces is below 2x the
-    reference walk's own error."""
+    mac 0 accepts a node by the group's box distance; mac 1 also accepts one
+    that passes every member's own MAC and holds no member.  Tolerances: the
+    group walk's RMS relative error against the direct sum is at most 1.05x the
+    reference walk's + 2e-6 (FP32 rounding), and its RMS relative difference
+    from the reference walk's forces is below 2x the reference walk's own
+    error."""
     m, q = plummer(4096, seed=1)
-    theta, eps = 0.5, 0.01
+    eps = 0.01
     s = build(bh, m, q, order=order, group_size=group_size)
-    f = s.walk(order=order, precision=precision, theta=theta, eps=eps, group_size=group_size)
+    f = s.walk(order=order, precision=precision, theta=theta, eps=eps, group_size=group_size,
+               mac=mac)
     s.sync()
     f = f.view(3, -1).T.cpu().numpy()
     fd = oracle_mod.direct_forces(m, *xyz(q), 1.0, eps * eps)
