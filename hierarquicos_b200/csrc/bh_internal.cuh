@@ -111,7 +111,7 @@ struct Buffers {
   // walk
   int32_t *wstack = nullptr;
   int64_t wstack_cap = 0;   // entries per warp slot
-  int64_t wstack_slots = 0; // warp slots: the walk launches wstack_slots / 4 blocks of 4 warps
+  int64_t wstack_slots = 0; // stacks: the walk launches at most this many one-warp blocks
   int32_t *counters = nullptr;   // [0] group cursor
   unsigned long long *stats = nullptr;  // interaction counters
   Scalars *sc = nullptr;

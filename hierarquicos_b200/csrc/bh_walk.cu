@@ -33,12 +33,10 @@ namespace bh {
 
 namespace {
 
-constexpr int kWalkWarps = 4;
-// resident blocks per SM the FP32 walk is compiled for (register budget)
-#ifndef BH_WALK_MIN_BLOCKS
-#define BH_WALK_MIN_BLOCKS 4
-#endif
-template <typename T> constexpr int walk_min_blocks() { return sizeof(T) == 4 ? BH_WALK_MIN_BLOCKS : 1; }
+// The walk runs one warp per block.  The FP32 walk is compiled for 16 resident
+// blocks per SM (128 registers a thread).
+constexpr int kWalkBlocksPerSm = 16;
+template <typename T> constexpr int walk_min_blocks() { return sizeof(T) == 4 ? kWalkBlocksPerSm : 1; }
 constexpr int kCellQ = 64;
 constexpr int kBodyPerLane = 16;
 constexpr int kBodyQ = 32 + kWarp * kBodyPerLane;  // 544
@@ -714,16 +712,15 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
   }
 }
 
-// Persistent warps take groups from a global cursor.  With 64-body groups a
-// group of <= 32 bodies runs the one-target-per-lane path.
+// Persistent warps, one per block, take groups from a global cursor until
+// none is left; block b uses stack slot b.  With 64-body groups a group of
+// <= 32 bodies runs the one-target-per-lane path.
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
-__global__ void __launch_bounds__(kWalkWarps * kWarp, walk_min_blocks<T>())
+__global__ void __launch_bounds__(kWarp, walk_min_blocks<T>())
 group_walk_kernel(WalkArgs a) {
-  __shared__ WarpSmem<T, ORDER> shm[kWalkWarps];
-  const int lane = threadIdx.x & (kWarp - 1), wid = threadIdx.x / kWarp;
-  WarpSmem<T, ORDER> &S = shm[wid];
-  const int64_t slot = (int64_t)blockIdx.x * kWalkWarps + wid;
-  int32_t *stack = a.stack + slot * a.stack_cap;
+  __shared__ WarpSmem<T, ORDER> S;
+  const int lane = threadIdx.x;
+  int32_t *stack = a.stack + (int64_t)blockIdx.x * a.stack_cap;
   const int stack_cap = (int)a.stack_cap;
   const int ngroups = a.sc->n_groups;
   const T theta2 = (T)a.theta2;
@@ -902,24 +899,39 @@ reference_walk_kernel(WalkArgs a, const int64_t *__restrict__ targets, int64_t n
   }
 }
 
-int g_sm_count = 0;
+int g_sm_count[64] = {0};
+
+int sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (g_sm_count[dev] == 0) {
+    int c = 0;
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+    g_sm_count[dev] = c > 0 ? c : 148;
+  }
+  return g_sm_count[dev];
+}
 
 }  // namespace
 
-int64_t walk_slots() {
-  if (g_sm_count == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sm_count <= 0) g_sm_count = 148;
-  }
-  return (int64_t)g_sm_count * 8 * kWalkWarps;
-}
+// stack slots: one per resident walk block of the FP32 walk (the most of any
+// instantiation)
+int64_t walk_slots() { return (int64_t)sm_count() * kWalkBlocksPerSm; }
 
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
 static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
-  const int blocks = (int)(a.slots / kWalkWarps);
-  group_walk_kernel<T, ORDER, MAXTPL, SOFT><<<blocks, kWalkWarps * kWarp, 0, s>>>(a);
+  // exactly the blocks that are resident at once: no block waits for a
+  // second wave behind the walk (which would also hold back other streams)
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int v = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, group_walk_kernel<T, ORDER, MAXTPL, SOFT>,
+                                                  kWarp, 0);
+    per_sm = v > 0 ? v : 1;
+  }
+  int64_t blocks = (int64_t)per_sm * sm_count();
+  if (blocks > a.slots) blocks = a.slots;
+  group_walk_kernel<T, ORDER, MAXTPL, SOFT><<<(unsigned)blocks, kWarp, 0, s>>>(a);
 }
 
 static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *out) {

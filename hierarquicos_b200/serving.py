@@ -43,7 +43,9 @@ from .system import BHSystem, _dptr
 
 STATE_BYTES_PER_BODY = 8 + 24 + 24          # m, q, p (FP64)
 RESIDENT_BYTES_PER_BODY = 2 * STATE_BYTES_PER_BODY + 24 + 24  # + tick copy, forces, coefficients
-WORKSPACE_BYTES_PER_BODY = 520              # engine workspace (keys, sort, tree, moments, groups)
+# engine workspace (keys, sort, tree, moments, groups: 520) + the lane's two
+# state buffers and forces (136)
+WORKSPACE_BYTES_PER_BODY = 656
 
 _ids = itertools.count()
 
@@ -95,19 +97,38 @@ class Request:
         return self._done.wait(timeout)
 
 
+_ROWS = ("m", "x", "y", "z", "px", "py", "pz")
+
+
 class _Lane:
+    """One host thread and its device buffers, all allocated once: the engine
+    workspace, two (7, max_tick_bodies) state buffers used in turn (m, x, y,
+    z, px, py, pz of every active system, back to back), the forces of a tick
+    and the per-system offsets and kick coefficients.  A tick gathers the
+    systems still running and the newly admitted ones into the other state
+    buffer, so the tick itself allocates no device memory."""
+
     def __init__(self, server: "Server", index: int):
         self.server = server
         self.index = index
         dev = server.device
+        cap, cap_s = server.max_tick_bodies, server.max_tick_systems
         with torch.cuda.device(dev):
             self.stream = torch.cuda.Stream(dev)
             self.h2d = torch.cuda.Stream(dev)
             self.d2h = torch.cuda.Stream(dev)
-        # the lane's workspace, allocated once for its largest tick
-        self.sys = BHSystem(dev.index).reserve(server.max_tick_bodies, server.max_tick_systems)
+            self.sys = BHSystem(dev.index).reserve(cap, cap_s)
+            self.buf = [torch.empty(7, cap, dtype=torch.float64, device=dev) for _ in range(2)]
+            self.out = torch.empty(3 * cap, dtype=torch.float64, device=dev)
+            self.d_off = torch.empty(cap_s + 1, dtype=torch.int64, device=dev)
+            self.d_coef = torch.empty(3 * cap_s, dtype=torch.float64, device=dev)
+        self.h_off = torch.empty(cap_s + 1, dtype=torch.int64, pin_memory=True)
+        self.h_coef = torch.empty(3 * cap_s, dtype=torch.float64, pin_memory=True)
+        self.cur = 0                       # buffer holding the running systems
+        self.pos: dict[int, int] = {}      # request id -> its first body in buf[cur]
+        self.d2h_done: torch.cuda.Event | None = None
         self.active: list[Request] = []
-        self.state: dict[int, dict] = {}
+        self.fresh: list[Request] = []     # admitted, not yet in a state buffer
         self.done_q: collections.deque = collections.deque()
         self.done_cv = threading.Condition()
         self.ticks = 0
@@ -119,100 +140,117 @@ class _Lane:
         self.finisher = threading.Thread(target=self._finish_loop, name=f"bh-done-{index}",
                                          daemon=True)
 
-    # -- staging --
-    def _stage(self, r: Request):
-        dev = self.server.device
-        host = r._pinned
-        if r.on_device:
-            self.state[r.id] = host
-            return
-        with torch.cuda.stream(self.h2d):
-            d = {k: v.to(dev, non_blocking=True) for k, v in host.items()}
-            ev = torch.cuda.Event()
-            ev.record(self.h2d)
-        self.stream.wait_event(ev)
-        for v in d.values():
-            v.record_stream(self.stream)
-        self.state[r.id] = d
+    def close(self):
+        """Frees the lane's device memory (after its threads have ended)."""
+        self.sys.close()
+        self.buf = []
+        self.out = self.d_off = self.d_coef = None
 
     # -- one tick: forces of every active system, then the per-system kicks --
     def _tick(self):
         srv = self.server
-        act = self.active
-        dev = srv.device
+        act = self.active + self.fresh
         sizes = [r.n for r in act]
         off = np.zeros(len(act) + 1, np.int64)
         off[1:] = np.cumsum(sizes)
         n = int(off[-1])
+        src, dst = self.buf[self.cur], self.buf[1 - self.cur]
         t_host = time.perf_counter()
         ev_begin = torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(self.stream):
             ev_begin.record(self.stream)
-            st = [self.state[r.id] for r in act]
-            cat = {k: torch.cat([s[k] for s in st]) for k in ("m", "x", "y", "z", "px", "py", "pz")}
-            out = torch.empty(3 * n, dtype=torch.float64, device=dev)
-            self.sys.forces_batch(cat["m"], cat["x"], cat["y"], cat["z"], off, srv.params, out=out)
-            coef = np.zeros((len(act), 3))
+            if self.d2h_done is not None:  # the previous results have left `out` and `dst`
+                self.stream.wait_event(self.d2h_done)
+            # host inputs of new requests: copied on the copy stream straight
+            # into their place in the new state buffer
+            host_new = [(i, r) for i, r in enumerate(act) if r in self.fresh and not r.on_device]
+            if host_new:
+                self.h2d.wait_event(ev_begin)
+                with torch.cuda.stream(self.h2d):
+                    for i, r in host_new:
+                        a, b = int(off[i]), int(off[i + 1])
+                        for k, name in enumerate(_ROWS):
+                            if name in r._pinned:
+                                dst[k, a:b].copy_(r._pinned[name], non_blocking=True)
+                    ev_in = torch.cuda.Event()
+                    ev_in.record(self.h2d)
             for i, r in enumerate(act):
-                if r.kind == "leapfrog":
-                    h = 0.5 * r.dt
-                    k = r._evals
-                    coef[i] = (0.0, h, r.dt) if k == 0 else ((h, h, r.dt) if k < r.steps
-                                                             else (h, 0.0, 0.0))
-                r._evals += 1
-            if any(r.kind == "leapfrog" for r in act):
-                d_coef = torch.as_tensor(coef.ravel(), device=dev)
-                d_off = torch.as_tensor(off, device=dev)
+                a, b = int(off[i]), int(off[i + 1])
+                if r.id in self.pos:                      # running: its current state
+                    p0 = self.pos[r.id]
+                    dst[:, a:b].copy_(src[:, p0:p0 + r.n], non_blocking=True)
+                elif r.on_device:                         # new, device inputs
+                    for k, name in enumerate(_ROWS):
+                        if name in r._pinned:
+                            dst[k, a:b].copy_(r._pinned[name], non_blocking=True)
+                if r.kind == "force" and r.id not in self.pos:
+                    dst[4:7, a:b].zero_()                 # no momenta: the kick is a no-op
+            if host_new:
+                self.stream.wait_event(ev_in)
+            out = self.out[:3 * n]
+            self.sys.forces_batch(dst[0, :n], dst[1, :n], dst[2, :n], dst[3, :n], off, srv.params,
+                                  out=out)
+            leap = [r.kind == "leapfrog" for r in act]
+            if any(leap):
+                coef = self.h_coef.numpy()
+                for i, r in enumerate(act):
+                    c = (0.0, 0.0, 0.0)
+                    if r.kind == "leapfrog":
+                        h = 0.5 * r.dt
+                        k = r._evals
+                        c = (0.0, h, r.dt) if k == 0 else ((h, h, r.dt) if k < r.steps
+                                                           else (h, 0.0, 0.0))
+                    coef[3 * i:3 * i + 3] = c
+                self.h_off.numpy()[:len(act) + 1] = off
+                self.d_coef[:3 * len(act)].copy_(self.h_coef[:3 * len(act)], non_blocking=True)
+                self.d_off[:len(act) + 1].copy_(self.h_off[:len(act) + 1], non_blocking=True)
                 check(lib().bh_kick_drift_systems(
-                    _dptr(cat["m"]), _dptr(out), _dptr(cat["x"]), _dptr(cat["y"]),
-                    _dptr(cat["z"]), _dptr(cat["px"]), _dptr(cat["py"]), _dptr(cat["pz"]),
-                    _dptr(d_off), len(act), n, _dptr(d_coef), self.stream.cuda_stream))
+                    _dptr(dst[0]), _dptr(out), _dptr(dst[1]), _dptr(dst[2]), _dptr(dst[3]),
+                    _dptr(dst[4]), _dptr(dst[5]), _dptr(dst[6]), _dptr(self.d_off), len(act), n,
+                    _dptr(self.d_coef), self.stream.cuda_stream))
+            for r in act:
+                r._evals += 1
+            # device results: copied into the request's own buffers
+            finished, keep = [], []
+            for i, r in enumerate(act):
+                a, b = int(off[i]), int(off[i + 1])
+                if r._evals >= r.evals_needed:
+                    finished.append((r, a, b))
+                    if r.on_device:
+                        if r.kind == "force":
+                            r._dev_result["f"].copy_(out[3 * a:3 * b].view(3, b - a),
+                                                     non_blocking=True)
+                        else:
+                            for k, name in enumerate(_ROWS[1:], start=1):
+                                r._dev_result[name].copy_(dst[k, a:b], non_blocking=True)
+                else:
+                    keep.append((r, a))
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(self.stream)
         self.tick_log.append((time.perf_counter() - t_host, ev_begin, ev))
-        keep = []
-        finished = []
-        for i, r in enumerate(act):
-            a, b = int(off[i]), int(off[i + 1])
-            self.state[r.id] = {k: v[a:b] for k, v in cat.items()}
-            if r._evals >= r.evals_needed:
-                finished.append((r, a, b))
-            else:
-                keep.append(r)
-        dev_done = [(r, a, b) for r, a, b in finished if r.on_device]
-        finished = [(r, a, b) for r, a, b in finished if not r.on_device]
-        if dev_done:
-            with torch.cuda.stream(self.stream):
-                for r, a, b in dev_done:
-                    if r.kind == "force":
-                        r._dev_out = {"f": out[3 * a:3 * b].view(3, b - a)}
-                    else:
-                        r._dev_out = {k: cat[k][a:b] for k in ("x", "y", "z", "px", "py", "pz")}
-                    done = torch.cuda.Event()
-                    done.record(self.stream)
-                    with self.done_cv:
-                        self.done_q.append((r, done))
-                        self.done_cv.notify()
-        if finished:
+        # host results on the copy stream
+        host_done = [(r, a, b) for r, a, b in finished if not r.on_device]
+        if host_done:
             self.d2h.wait_event(ev)
             with torch.cuda.stream(self.d2h):
-                for r, a, b in finished:
+                for r, a, b in host_done:
                     if r.kind == "force":
                         r._host_out["f"].copy_(out[3 * a:3 * b], non_blocking=True)
                     else:
-                        for k in ("x", "y", "z", "px", "py", "pz"):
-                            r._host_out[k].copy_(cat[k][a:b], non_blocking=True)
-                    done = torch.cuda.Event()
-                    done.record(self.d2h)
-                    out.record_stream(self.d2h)
-                    for v in cat.values():
-                        v.record_stream(self.d2h)
-                    with self.done_cv:
-                        self.done_q.append((r, done))
-                        self.done_cv.notify()
-        for r, _, _ in finished:
-            del self.state[r.id]
-        self.active = keep
+                        for k, name in enumerate(_ROWS[1:], start=1):
+                            r._host_out[name].copy_(dst[k, a:b], non_blocking=True)
+                self.d2h_done = torch.cuda.Event()
+                self.d2h_done.record(self.d2h)
+        with self.done_cv:
+            for r, a, b in finished:
+                done = torch.cuda.Event()
+                done.record(self.d2h if not r.on_device else self.stream)
+                self.done_q.append((r, done))
+            self.done_cv.notify()
+        self.cur = 1 - self.cur
+        self.pos = {r.id: a for r, a in keep}
+        self.active = [r for r, _ in keep]
+        self.fresh = []
         self.ticks += 1
         self.tick_bodies += n
 
@@ -221,11 +259,8 @@ class _Lane:
         torch.cuda.set_device(srv.device)
         try:
             while True:
-                new = srv._admit(self)
-                for r in new:
-                    self._stage(r)
-                self.active.extend(new)
-                if not self.active:
+                self.fresh = srv._admit(self)
+                if not self.active and not self.fresh:
                     if srv._stopping and srv._idle():
                         break
                     with srv._cv:
@@ -233,12 +268,13 @@ class _Lane:
                     continue
                 self._tick()
         except Exception as e:  # a failed tick fails its requests, not the server
-            for r in self.active:
+            for r in self.active + self.fresh:
                 r.error = str(e)
                 r.t_done = time.perf_counter()
                 srv._release(r)
                 r._done.set()
             self.active = []
+            self.fresh = []
             srv._lane_error = e
         finally:
             with self.done_cv:
@@ -258,7 +294,7 @@ class _Lane:
             ev.synchronize()
             r.t_done = time.perf_counter()
             if r.on_device:
-                do = r._dev_out
+                do = r._dev_result
                 if r.kind == "force":
                     r.forces = do["f"].T
                 else:
@@ -342,16 +378,17 @@ class Server:
     @staticmethod
     def _pin(r: Request):
         if r.on_device:
+            # the inputs are read in place; the result buffers are allocated
+            # here, on the client's thread, so a lane's tick allocates nothing
             q = r.q if r.q.shape[0] == 3 else r.q.T
-            d = {"m": r.m.contiguous(), "x": q[0].contiguous(), "y": q[1].contiguous(),
-                 "z": q[2].contiguous()}
+            d = {"m": r.m, "x": q[0], "y": q[1], "z": q[2]}
+            dev, f64 = r.m.device, torch.float64
             if r.kind == "leapfrog":
                 p = r.p if r.p.shape[0] == 3 else r.p.T
-                d.update(px=p[0].clone(), py=p[1].clone(), pz=p[2].clone())
-                d.update(x=d["x"].clone(), y=d["y"].clone(), z=d["z"].clone())
+                d.update(px=p[0], py=p[1], pz=p[2])
+                r._dev_result = {k: torch.empty(r.n, dtype=f64, device=dev) for k in _ROWS[1:]}
             else:
-                z = torch.zeros(r.n, dtype=torch.float64, device=r.m.device)
-                d.update(px=z, py=z, pz=z)
+                r._dev_result = {"f": torch.empty(3, r.n, dtype=f64, device=dev)}
             r._pinned = d
             return
 
@@ -369,8 +406,6 @@ class Server:
             r._host_out = {k: torch.empty(r.n, dtype=torch.float64, pin_memory=True)
                            for k in ("x", "y", "z", "px", "py", "pz")}
         else:
-            z = torch.zeros(r.n, dtype=torch.float64, pin_memory=True)
-            host.update(px=z, py=z, pz=z)
             r._host_out = {"f": torch.empty(3 * r.n, dtype=torch.float64, pin_memory=True)}
         r._pinned = host
 
@@ -403,6 +438,11 @@ class Server:
                 ln.thread.join()
             if ln.finisher.is_alive():
                 ln.finisher.join()
+        # free the lanes' device memory now, at a known point, rather than
+        # whenever the garbage collector reaches the server
+        torch.cuda.synchronize(self.device)
+        for ln in self.lanes:
+            ln.close()
 
     def __enter__(self):
         return self.start()

@@ -131,3 +131,46 @@ def test_refuses_requests_that_cannot_fit(sv):
         srv.submit(sv.Request("force", m, q))
     with pytest.raises(ValueError):
         sv.Request("leapfrog", m, q, None, steps=3)
+
+
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_device_requests_match_plain_path(sv, lanes):
+    """Device-resident requests (CUDA tensors in, CUDA tensors out), mixed with
+    host requests and leapfrog runs of different lengths that join and leave
+    while others run: every result equals the plain path's bit for bit."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    host = mixed_requests(sv, 6, seed=5)
+    dev_reqs, ref = [], []
+    for k in range(6):
+        n = [700, 3000, 12000, 5000, 900, 20000][k]
+        if k % 2 == 0:
+            m, q, _ = ic(n, 500 + k, profile="hernquist")
+            dev_reqs.append(sv.Request("force", torch.as_tensor(m, device=dev),
+                                       torch.as_tensor(q.T.copy(), device=dev)))
+            ref.append(("force", m, q))
+        else:
+            m, q, p = ic(n, 500 + k, velocities=True)
+            steps = 2 + k
+            dev_reqs.append(sv.Request("leapfrog", torch.as_tensor(m, device=dev),
+                                       torch.as_tensor(q, device=dev),
+                                       torch.as_tensor(p, device=dev), steps=steps, dt=1e-3))
+            ref.append(("leapfrog", m, q, p, steps))
+    with sv.Server(lanes=lanes, max_tick_bodies=1 << 16, hbm_budget=40e9, **PARAMS) as srv:
+        for a, b in zip(host, dev_reqs):
+            srv.submit(a)
+            srv.submit(b)
+        srv.drain(timeout=300)
+    for r in host:
+        assert r.error is None
+        check_against_plain(r)
+    for r, e in zip(dev_reqs, ref):
+        assert r.error is None
+        if e[0] == "force":
+            assert r.forces.is_cuda and r.forces.shape == (r.n, 3)
+            assert np.array_equal(r.forces.cpu().numpy(), plain_forces(e[1], e[2]))
+        else:
+            qe, pe = plain_leapfrog(e[1], e[2], e[3], e[4], 1e-3)
+            assert np.array_equal(r.q_out.cpu().numpy(), qe)
+            assert np.array_equal(r.p_out.cpu().numpy(), pe)
