@@ -301,7 +301,7 @@ void enqueue_build(bh_system *s, int keys_from_scalars, cudaStream_t st) {
   else
     bh::launch_keys(s->m, s->x, s->y, s->z, n, L, p.amp, p.com_mode, b, st);
   const int bits = (L == 0) ? 3 * bh::kMaxDepth : 3 * L;
-  bh::radix_sort_pairs(b.k0, b.v0, b.k1, b.v1, n, nullptr, bits, b.hist, st);
+  bh::radix_sort_pairs(b.k0, b.v0, b.k1, b.v1, n, nullptr, bits, b.hist, &b.sc->err, st);
   bh::launch_sort_by_system(n, b, st);
   if (L == 0) bh::launch_auto_depth(n, b, st);
   bh::launch_gather(s->m, s->x, s->y, s->z, n, b, st);

@@ -144,14 +144,15 @@ inline int grid_for(int64_t n, int threads, int cap) {
 
 // stable LSD radix sort of (key, value) pairs over bits [0, bits); the
 // result ends in (k0, v0).  n_dev, when given, holds the element count on the
-// device (n is then an upper bound).
+// device (n is then an upper bound).  A look-back wait that gives up sets
+// kErrIndex in *err (device).
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
-                      const int32_t *n_dev, int bits, int32_t *hist, cudaStream_t s);
-// count table of the radix sort (256 digits x 4096-key tiles) + its scan
-// scratch, in int32 entries
+                      const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s);
+// scratch of the radix sort, in int32 entries: digit counts of 8 passes x 256
+// digits, 8 tile counters, and a 64-bit word per (pass, 4096-key tile, digit)
 constexpr int64_t scan_tmp_entries(int64_t n) { return (n + 8191) / 8192 + 2; }
 constexpr int64_t radix_hist_entries(int64_t n) {
-  return 256 * ((n + 4095) / 4096) + 1 + scan_tmp_entries(256 * ((n + 4095) / 4096));
+  return 8 * 256 + 8 + 2 * 8 * 256 * ((n + 4095) / 4096 + 1);
 }
 
 // exclusive scan of n int32 values; total written to *total (device) if given

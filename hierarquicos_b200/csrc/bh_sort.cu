@@ -6,13 +6,17 @@
 // exactly the stable sort's permutation: equal keys keep ascending original
 // index, as the merge sort's "ties take the left element" rule (:537-538).
 //
-// Each pass (8-bit digit): an upsweep counts digits per 4096-key tile, one
-// exclusive scan over the digit-major count table gives every (digit, tile)
-// its output base, and a downsweep ranks keys inside the tile with warp
-// __match_any_sync / popc ranking (element order = warp, iteration, lane, so
-// ranks are stable), stages the tile in shared memory in digit order and
-// writes it out so that runs of equal digits land on consecutive addresses.
-// No pass waits on another block: there is no spin wait anywhere.
+// Digit counts of every pass come from one histogram kernel over the keys;
+// each pass (8-bit digit) is then ONE kernel with decoupled look-back: a block
+// claims the next 4096-key tile from an atomic counter, ranks its keys inside
+// the tile with warp __match_any_sync / popc ranking (element order = warp,
+// iteration, lane, so ranks are stable), publishes its per-digit counts, adds
+// up the counts of the tiles before it (each tile's word holds either its own
+// count or, once known, the inclusive prefix of all tiles up to it), stages
+// the tile in shared memory in digit order and writes it out so that runs of
+// equal digits land on consecutive addresses.  A block only waits for tiles
+// claimed before its own, by blocks that are already running; every wait is
+// bounded and a wait that gives up raises an error flag instead of hanging.
 #include "bh_internal.cuh"
 
 namespace bh {
@@ -24,6 +28,7 @@ constexpr int kSortWarps = kSortThreads / kWarp;
 constexpr int kItems = 16;
 constexpr int kTile = kSortThreads * kItems;  // 4096 keys per block
 constexpr int kRadix = 256;
+constexpr int kMaxPasses = 8;  // 64-bit keys
 
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
@@ -65,54 +70,87 @@ __device__ int block_excl_scan(int v, int *ws, int *total) {
   return off + incl - v;
 }
 
+// Digit histograms of all passes: ghist[p][d] = number of keys whose digit p
+// is d (warp-aggregated shared-memory counts, then one global add per bin).
 __global__ void __launch_bounds__(kSortThreads)
-upsweep_kernel(const uint64_t *__restrict__ keys, int64_t n_max, const int32_t *n_dev, int shift,
-               int32_t *__restrict__ hist, int nblocks) {
-  __shared__ int wh[kSortWarps][kRadix];
-  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+digit_hist_kernel(const uint64_t *__restrict__ keys, int64_t n_max, const int32_t *n_dev,
+                  int passes, uint32_t *__restrict__ ghist) {
+  __shared__ uint32_t h[kMaxPasses][kRadix];
+  const int lane = threadIdx.x & (kWarp - 1);
   const int64_t n = n_dev ? bh_min64(n_max, (int64_t)*n_dev) : n_max;
-  for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&wh[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kSortThreads) (&h[0][0])[i] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kTile + warp * kWarp * kItems;
-#pragma unroll 4
-  for (int i = 0; i < kItems; ++i) {
-    int64_t idx = base + i * kWarp + lane;
-    if (idx < n) atomicAdd(&wh[warp][(int)((keys[idx] >> shift) & 0xff)], 1);
+  const unsigned lt = lanemask_lt();
+  const int64_t stride = (int64_t)gridDim.x * kSortThreads;
+  for (int64_t base = (int64_t)blockIdx.x * kSortThreads; base < n; base += stride) {
+    const int64_t idx = base + threadIdx.x;
+    const bool valid = idx < n;
+    const uint64_t k = valid ? keys[idx] : 0ull;
+    for (int p = 0; p < passes; ++p) {
+      const int d = valid ? (int)((k >> (8 * p)) & 0xff) : kRadix;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      if (d < kRadix && (peers & lt) == 0) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    }
+    (void)lane;
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
-    int s = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) s += wh[w][d];
-    hist[(int64_t)d * nblocks + blockIdx.x] = s;
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t c = h[p][threadIdx.x];  // kSortThreads == kRadix
+    if (c) atomicAdd(&ghist[p * kRadix + threadIdx.x], c);
   }
 }
 
-struct DownSmem {
+// Exclusive scan of each pass's 256 digit counts, in place.
+__global__ void __launch_bounds__(kSortThreads) digit_scan_kernel(uint32_t *ghist, int passes) {
+  __shared__ int ws[kSortWarps];
+  for (int p = 0; p < passes; ++p) {
+    const int v = (int)ghist[p * kRadix + threadIdx.x];
+    const int ex = block_excl_scan(v, ws, nullptr);
+    ghist[p * kRadix + threadIdx.x] = (uint32_t)ex;
+  }
+}
+
+// tile words: top 2 bits the state, low 62 bits the count
+constexpr uint64_t kTileAggregate = 1ull << 62;  // the tile's own count
+constexpr uint64_t kTileInclusive = 2ull << 62;  // sum of the counts of tiles 0..t
+constexpr uint64_t kTileValue = (1ull << 62) - 1;
+constexpr int64_t kLookbackSpins = 1 << 22;     // per word; about a second at most
+
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+struct PassSmem {
   uint64_t sk[kTile];
   int32_t sv[kTile];
   int wh[kSortWarps][kRadix];
   int tile_start[kRadix];
   int gbase[kRadix];
   int ws[kSortWarps];
+  int tile;
 };
 
 __global__ void __launch_bounds__(kSortThreads)
-downsweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vin,
-                 uint64_t *__restrict__ kout, int32_t *__restrict__ vout, int64_t n_max,
-                 const int32_t *n_dev, int shift, const int32_t *__restrict__ hist, int nblocks) {
+onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vin,
+                uint64_t *__restrict__ kout, int32_t *__restrict__ vout, int64_t n_max,
+                const int32_t *n_dev, int shift, const uint32_t *__restrict__ gofs,
+                uint64_t *__restrict__ tiles, int32_t *__restrict__ tile_ctr, int *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  DownSmem &S = *reinterpret_cast<DownSmem *>(smem_raw);
+  PassSmem &S = *reinterpret_cast<PassSmem *>(smem_raw);
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
-  const int64_t n = n_dev ? bh_min64(n_max, (int64_t)*n_dev) : n_max;
-  const int64_t tile_base = (int64_t)blockIdx.x * kTile;
-  if (tile_base >= n) return;  // uniform across the block
-  const int tile_n = (int)bh_min64(kTile, n - tile_base);
-
+  if (threadIdx.x == 0) S.tile = atomicAdd(tile_ctr, 1);
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
-  for (int d = threadIdx.x; d < kRadix; d += kSortThreads)
-    S.gbase[d] = hist[(int64_t)d * nblocks + blockIdx.x];
   __syncthreads();
+  const int t = S.tile;
+  const int64_t n = n_dev ? bh_min64(n_max, (int64_t)*n_dev) : n_max;
+  const int64_t tile_base = (int64_t)t * kTile;
+  if (tile_base >= n) return;  // uniform across the block; later tiles return too
+  const int tile_n = (int)bh_min64(kTile, n - tile_base);
 
   uint64_t k[kItems];
   int32_t v[kItems];
@@ -139,27 +177,45 @@ downsweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ v
     rank[i] = pre + rin;
   }
   __syncthreads();
-  // per digit: exclusive offsets of the warps, tile count
+  // per digit (thread d): exclusive offsets of the warps and the tile's count
+  const int d = threadIdx.x;  // kSortThreads == kRadix
   int cnt = 0;
-  {
-    const int d = threadIdx.x;  // kSortThreads == kRadix
-    int run = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-      int c = S.wh[w][d];
-      S.wh[w][d] = run;
-      run += c;
-    }
-    cnt = run;
+  for (int w = 0; w < kSortWarps; ++w) {
+    const int c = S.wh[w][d];
+    S.wh[w][d] = cnt;
+    cnt += c;
   }
+  // publish, then look back over the earlier tiles for this digit
+  uint64_t *word = tiles + (int64_t)t * kRadix + d;
+  int64_t excl = 0;
+  if (t == 0) {
+    st_relaxed(word, kTileInclusive | (uint64_t)cnt);
+  } else {
+    st_relaxed(word, kTileAggregate | (uint64_t)cnt);
+    int j = t - 1;
+    int64_t spins = 0;
+    while (j >= 0) {
+      const uint64_t w = ld_relaxed(tiles + (int64_t)j * kRadix + d);
+      if ((w & ~kTileValue) == 0) {
+        if (++spins > kLookbackSpins) { atomicOr(err, kErrIndex); break; }
+        continue;
+      }
+      excl += (int64_t)(w & kTileValue);
+      if ((w & ~kTileValue) == kTileInclusive) break;
+      --j;
+    }
+    st_relaxed(word, kTileInclusive | (uint64_t)(excl + cnt));
+  }
+  S.gbase[d] = (int)(gofs[d] + excl);
   int start = block_excl_scan(cnt, S.ws, nullptr);
-  S.tile_start[threadIdx.x] = start;
+  S.tile_start[d] = start;
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
-    const int d = dig[i];
-    if (d < kRadix) {
-      int pos = S.tile_start[d] + S.wh[warp][d] + rank[i];
+    const int dd = dig[i];
+    if (dd < kRadix) {
+      int pos = S.tile_start[dd] + S.wh[warp][dd] + rank[i];
       S.sk[pos] = k[i];
       S.sv[pos] = v[i];
     }
@@ -167,8 +223,8 @@ downsweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ v
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
     uint64_t key = S.sk[j];
-    int d = (int)((key >> shift) & 0xff);
-    int64_t o = (int64_t)S.gbase[d] + (j - S.tile_start[d]);
+    int dd = (int)((key >> shift) & 0xff);
+    int64_t o = (int64_t)S.gbase[dd] + (j - S.tile_start[dd]);
     kout[o] = key;
     vout[o] = S.sv[j];
   }
@@ -268,7 +324,7 @@ bool g_sort_attr_set = false;
 
 }  // namespace
 
-static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256,
+static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256 && kMaxPasses == 8,
               "scan_tmp_entries / radix_hist_entries in bh_internal.cuh assume these sizes");
 
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
@@ -281,25 +337,32 @@ void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n
 }
 
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
-                      const int32_t *n_dev, int bits, int32_t *hist, cudaStream_t s) {
+                      const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s) {
   if (!g_sort_attr_set) {
-    cudaFuncSetAttribute(downsweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(DownSmem));
+    cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem));
     g_sort_attr_set = true;
   }
-  const int nblocks = (int)((n + kTile - 1) / kTile);
-  const int64_t entries = (int64_t)kRadix * nblocks;
-  // the scan's block sums live after the count table
-  int32_t *scan_tmp = hist + entries + 1;
+  const int64_t ntiles = (n + kTile - 1) / kTile;
   int passes = (bits + 7) / 8;
+  if (passes < 1) passes = 1;
+  if (passes > kMaxPasses) passes = kMaxPasses;
+  // scratch layout (int32 entries): digit counts [8][256], tile counters [8],
+  // then the tile words (uint64) [passes][ntiles][256]
+  uint32_t *ghist = reinterpret_cast<uint32_t *>(hist);
+  int32_t *ctr = hist + kMaxPasses * kRadix;
+  uint64_t *tiles = reinterpret_cast<uint64_t *>(hist + kMaxPasses * kRadix + kMaxPasses);
+  const int64_t used = kMaxPasses * kRadix + kMaxPasses + 2 * (int64_t)passes * ntiles * kRadix;
+  cudaMemsetAsync(hist, 0, used * sizeof(int32_t), s);
+  digit_hist_kernel<<<grid_for(n, kSortThreads, 148 * 8), kSortThreads, 0, s>>>(k0, n, n_dev,
+                                                                                passes, ghist);
+  digit_scan_kernel<<<1, kSortThreads, 0, s>>>(ghist, passes);
   uint64_t *ki = k0, *ko = k1;
   int32_t *vi = v0, *vo = v1;
   for (int p = 0; p < passes; ++p) {
-    int shift = 8 * p;
-    upsweep_kernel<<<nblocks, kSortThreads, 0, s>>>(ki, n, n_dev, shift, hist, nblocks);
-    exclusive_scan(hist, hist, entries, nullptr, nullptr, scan_tmp, s);
-    downsweep_kernel<<<nblocks, kSortThreads, sizeof(DownSmem), s>>>(ki, vi, ko, vo, n, n_dev,
-                                                                      shift, hist, nblocks);
+    onesweep_kernel<<<(unsigned)(ntiles > 0 ? ntiles : 1), kSortThreads, sizeof(PassSmem), s>>>(
+        ki, vi, ko, vo, n, n_dev, 8 * p, ghist + p * kRadix, tiles + (int64_t)p * ntiles * kRadix,
+        ctr + p, err);
     uint64_t *tk = ki; ki = ko; ko = tk;
     int32_t *tv = vi; vi = vo; vo = tv;
   }
@@ -309,8 +372,6 @@ void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int6
     cudaMemcpyAsync(v0, vi, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
   }
 }
-
-
 
 // The key sort orders all bodies of a batch by key; a stable sort by system
 // then restores the systems' ranges with each range in key order (LSD order:
@@ -325,7 +386,7 @@ void launch_sort_by_system(int64_t n, Buffers &b, cudaStream_t s) {
   int32_t *cv1 = b.bn_flag;                                      // scratch until the marks
   const int grid = grid_for(n, 256, 148 * 16);
   sys_keys_kernel<<<grid, 256, 0, s>>>(b.v0, b.sys_of, n, ck0, cv0);
-  radix_sort_pairs(ck0, cv0, ck1, cv1, n, nullptr, bits, b.hist, s);
+  radix_sort_pairs(ck0, cv0, ck1, cv1, n, nullptr, bits, b.hist, &b.sc->err, s);
   regather_kernel<<<grid, 256, 0, s>>>(b.k0, b.v0, cv0, n, b.k1, b.v1);
   cudaMemcpyAsync(b.k0, b.k1, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
   cudaMemcpyAsync(b.v0, b.v1, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);

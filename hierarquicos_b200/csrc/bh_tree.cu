@@ -279,7 +279,7 @@ void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s) {
   int32_t *cv1 = b.cn_parent;                                // scratch: filled later
   compact_keys_kernel<<<grid, 256, 0, s>>>(n, b.bn_flag, rank, b.bn_level, b.bn_first, first_bits,
                                            ck0, cv0);
-  radix_sort_pairs(ck0, cv0, ck1, cv1, n, total, first_bits + 5, b.hist, s);
+  radix_sort_pairs(ck0, cv0, ck1, cv1, n, total, first_bits + 5, b.hist, &b.sc->err, s);
   cudaMemcpyAsync(b.cn_bin, cv0, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
   cudaMemsetAsync(b.cn_parent, 0xff, n * sizeof(int32_t), s);  // roots keep -1
   bin2cn_kernel<<<grid, 256, 0, s>>>(b.cn_bin, b.sc, b.bin2cn);

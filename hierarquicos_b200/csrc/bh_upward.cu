@@ -12,6 +12,9 @@
 // Lone particles are point children (mass, position, no moments), so a node's
 // children are processed exactly like the reference's twig/leaf children.
 //
+// One launch per level, deepest first; a thread computes one node, loading
+// all of its child records before using any so that the loads overlap.
+//
 // The same pass writes the normalised FP32 copies used by the FP32 walk:
 // quadrupole / (M ssa^2) with its trace, octupole / (M ssa^3), where M is the
 // total mass and ssa the root cube side, so the walk's values are O(1)
@@ -22,109 +25,143 @@ namespace bh {
 
 namespace {
 
+__device__ __forceinline__ double4 ld_com(const double4 *p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2 *>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// One child's contribution to the moments about (cx, cy, cz): its own
+// moments (node children), then the parallel-axis and octupole cross terms.
 template <int ORDER>
-__global__ void __launch_bounds__(128)
-upward_level_kernel(int level, const int32_t *__restrict__ level_begin,
-                    const int4 *__restrict__ meta, const int32_t *__restrict__ child,
-                    const double4 *__restrict__ spos, const int32_t *__restrict__ sys_of,
-                    const SysScalars *__restrict__ sys,
-                    double4 *__restrict__ com, double *__restrict__ quad,
-                    double *__restrict__ oct, float4 *__restrict__ fq, float4 *__restrict__ fo) {
-  const int lb = level_begin[level], le = level_begin[level + 1];
-  for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x) {
-    const int4 mt = meta[j];  // first, count, level, nchild
-    const SysScalars &ss = sys[sys_of[mt.x]];
-    const double inv_m = 1.0 / ss.mass;
-    const double inv_s = 1.0 / ss.ssa;
-    const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
-    const bool bucket = (mt.w == 0);
-    const int nch = bucket ? mt.y : mt.w;
-    // pass 1: mass and centre of mass
-    double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
-    for (int c = 0; c < nch; ++c) {
-      double cm, px, py, pz;
-      if (bucket) {
-        double4 p = spos[mt.x + c];
-        cm = p.w; px = p.x; py = p.y; pz = p.z;
-      } else {
-        int32_t ch = child[8 * j + c];
-        if (ch < 0) {
-          double4 p = spos[~ch];
-          cm = p.w; px = p.x; py = p.y; pz = p.z;
-        } else {
-          double4 q = com[ch];
-          cm = q.w; px = q.x; py = q.y; pz = q.z;
-        }
-      }
-      M = M + cm;
-      cx = cx + cm * px;
-      cy = cy + cm * py;
-      cz = cz + cm * pz;
+__device__ __forceinline__ void add_child(double pm, double px, double py, double pz, bool node,
+                                          const double *Qd, const double *Od, double cx,
+                                          double cy, double cz, double *Q, double *O) {
+  const double dx = px - cx, dy = py - cy, dz = pz - cz;
+  if (node) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) Q[k] = Q[k] + Qd[k];
+    if (ORDER >= 8) {
+#pragma unroll
+      for (int k = 0; k < 14; ++k) O[k] = O[k] + Od[k];
+    }
+  }
+  Q[0] = Q[0] + pm * (dx * dx);
+  Q[1] = Q[1] + pm * (dy * dy);
+  Q[2] = Q[2] + pm * (dz * dz);
+  Q[3] = Q[3] + pm * dx * dy;
+  Q[4] = Q[4] + pm * dx * dz;
+  Q[5] = Q[5] + pm * dy * dz;
+  if (ORDER >= 8) {
+    O[0] = O[0] + pm * dx * (dx * dx);
+    O[1] = O[1] + pm * dx * (dy * dy);
+    O[2] = O[2] + pm * dx * (dz * dz);
+    O[3] = O[3] + pm * dy * (dx * dx);
+    O[4] = O[4] + pm * dy * (dy * dy);
+    O[5] = O[5] + pm * dy * (dz * dz);
+    O[6] = O[6] + pm * dz * (dx * dx);
+    O[7] = O[7] + pm * dz * (dy * dy);
+    O[8] = O[8] + pm * dz * (dz * dz);
+    O[9] = O[9] + pm * dx * dy * dz;
+    if (node) {
+      O[0] = O[0] + 3.0 * dx * Qd[0];
+      O[1] = O[1] + 2.0 * dy * Qd[3] + dx * Qd[1];
+      O[2] = O[2] + 2.0 * dz * Qd[4] + dx * Qd[2];
+      O[3] = O[3] + 2.0 * dx * Qd[3] + dy * Qd[0];
+      O[4] = O[4] + 3.0 * dy * Qd[1];
+      O[5] = O[5] + 2.0 * dz * Qd[5] + dy * Qd[2];
+      O[6] = O[6] + 2.0 * dx * Qd[4] + dz * Qd[0];
+      O[7] = O[7] + 2.0 * dy * Qd[5] + dz * Qd[1];
+      O[8] = O[8] + 3.0 * dz * Qd[2];
+      O[9] = O[9] + dx * Qd[5] + dy * Qd[4] + dz * Qd[3];
+    }
+  }
+}
+
+// Mass, centre of mass and moments of node j from its children.  For a node
+// with child entries, all child records are loaded before any is used, so the
+// loads overlap; the sums run in child order either way.
+template <int ORDER>
+__device__ void compute_node(int j, const int4 *__restrict__ meta, const int32_t *__restrict__ child,
+                             const double4 *__restrict__ spos, const int32_t *__restrict__ sys_of,
+                             const SysScalars *__restrict__ sys, double4 *com, double *quad,
+                             double *oct, float4 *__restrict__ fq, float4 *__restrict__ fo) {
+  const int4 mt = meta[j];  // first, count, level, nchild
+  const SysScalars &ss = sys[sys_of[mt.x]];
+  const double inv_m = 1.0 / ss.mass;
+  const double inv_s = 1.0 / ss.ssa;
+  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
+  double M = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+  double Q[6] = {0, 0, 0, 0, 0, 0};
+  double O[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (mt.w == 0) {  // bucket of identical keys: its bodies are the children
+    for (int c = 0; c < mt.y; ++c) {
+      const double4 p = spos[mt.x + c];
+      M = M + p.w;
+      cx = cx + p.w * p.x;
+      cy = cy + p.w * p.y;
+      cz = cz + p.w * p.z;
     }
     cx = cx / M; cy = cy / M; cz = cz / M;
     com[j] = make_double4(cx, cy, cz, M);
-    if (ORDER < 4) continue;
-    // pass 2: moments about (cx, cy, cz)
-    double Q[6] = {0, 0, 0, 0, 0, 0};
-    double O[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < nch; ++c) {
-      double pm, px, py, pz;
-      int32_t node = -1;
-      if (bucket) {
-        double4 p = spos[mt.x + c];
-        pm = p.w; px = p.x; py = p.y; pz = p.z;
-      } else {
-        int32_t ch = child[8 * j + c];
-        if (ch < 0) {
-          double4 p = spos[~ch];
-          pm = p.w; px = p.x; py = p.y; pz = p.z;
-        } else {
-          double4 q = com[ch];
-          pm = q.w; px = q.x; py = q.y; pz = q.z;
-          node = ch;
-        }
+    if constexpr (ORDER < 4) {
+      return;
+    } else {
+      for (int c = 0; c < mt.y; ++c) {
+        const double4 p = spos[mt.x + c];
+        add_child<ORDER>(p.w, p.x, p.y, p.z, false, nullptr, nullptr, cx, cy, cz, Q, O);
       }
-      const double dx = px - cx, dy = py - cy, dz = pz - cz;
-      double Qd[6];
-      if (node >= 0) {
+    }
+  } else {
+    const int4 c0 = *reinterpret_cast<const int4 *>(child + 8 * (int64_t)j);
+    const int4 c1 = *reinterpret_cast<const int4 *>(child + 8 * (int64_t)j + 4);
+    const int32_t ch[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    double4 cd[8];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) { Qd[k] = quad[6 * (int64_t)node + k]; Q[k] = Q[k] + Qd[k]; }
-        if (ORDER >= 8) {
+    for (int c = 0; c < 8; ++c) {
+      cd[c] = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (c < mt.w) cd[c] = ch[c] < 0 ? spos[~ch[c]] : ld_com(com + ch[c]);
+    }
+    double Qd[ORDER >= 4 ? 8 : 1][6];
+    if (ORDER >= 4) {
 #pragma unroll
-          for (int k = 0; k < 14; ++k) O[k] = O[k] + oct[14 * (int64_t)node + k];
-        }
-      }
-      Q[0] = Q[0] + pm * (dx * dx);
-      Q[1] = Q[1] + pm * (dy * dy);
-      Q[2] = Q[2] + pm * (dz * dz);
-      Q[3] = Q[3] + pm * dx * dy;
-      Q[4] = Q[4] + pm * dx * dz;
-      Q[5] = Q[5] + pm * dy * dz;
-      if (ORDER >= 8) {
-        O[0] = O[0] + pm * dx * (dx * dx);
-        O[1] = O[1] + pm * dx * (dy * dy);
-        O[2] = O[2] + pm * dx * (dz * dz);
-        O[3] = O[3] + pm * dy * (dx * dx);
-        O[4] = O[4] + pm * dy * (dy * dy);
-        O[5] = O[5] + pm * dy * (dz * dz);
-        O[6] = O[6] + pm * dz * (dx * dx);
-        O[7] = O[7] + pm * dz * (dy * dy);
-        O[8] = O[8] + pm * dz * (dz * dz);
-        O[9] = O[9] + pm * dx * dy * dz;
-        if (node >= 0) {
-          O[0] = O[0] + 3.0 * dx * Qd[0];
-          O[1] = O[1] + 2.0 * dy * Qd[3] + dx * Qd[1];
-          O[2] = O[2] + 2.0 * dz * Qd[4] + dx * Qd[2];
-          O[3] = O[3] + 2.0 * dx * Qd[3] + dy * Qd[0];
-          O[4] = O[4] + 3.0 * dy * Qd[1];
-          O[5] = O[5] + 2.0 * dz * Qd[5] + dy * Qd[2];
-          O[6] = O[6] + 2.0 * dx * Qd[4] + dz * Qd[0];
-          O[7] = O[7] + 2.0 * dy * Qd[5] + dz * Qd[1];
-          O[8] = O[8] + 3.0 * dz * Qd[2];
-          O[9] = O[9] + dx * Qd[5] + dy * Qd[4] + dz * Qd[3];
+      for (int c = 0; c < 8; ++c) {
+        if (c < mt.w && ch[c] >= 0) {
+          const double2 *q2 = reinterpret_cast<const double2 *>(quad + 6 * (int64_t)ch[c]);
+          const double2 a = __ldcg(q2), b = __ldcg(q2 + 1), e = __ldcg(q2 + 2);
+          Qd[c][0] = a.x; Qd[c][1] = a.y; Qd[c][2] = b.x; Qd[c][3] = b.y; Qd[c][4] = e.x; Qd[c][5] = e.y;
         }
       }
     }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      if (c < mt.w) {
+        M = M + cd[c].w;
+        cx = cx + cd[c].w * cd[c].x;
+        cy = cy + cd[c].w * cd[c].y;
+        cz = cz + cd[c].w * cd[c].z;
+      }
+    }
+    cx = cx / M; cy = cy / M; cz = cz / M;
+    com[j] = make_double4(cx, cy, cz, M);
+    if constexpr (ORDER < 4) {
+      return;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < mt.w) {
+          double Od[14];
+          if (ORDER >= 8 && ch[c] >= 0) {
+#pragma unroll
+            for (int k = 0; k < 14; ++k) Od[k] = __ldcg(oct + 14 * (int64_t)ch[c] + k);
+          }
+          add_child<ORDER>(cd[c].w, cd[c].x, cd[c].y, cd[c].z, ch[c] >= 0, Qd[c], Od, cx, cy, cz,
+                           Q, O);
+        }
+      }
+    }
+  }
+  if constexpr (ORDER >= 4) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) quad[6 * (int64_t)j + k] = Q[k];
     const double trq = Q[0] + Q[1] + Q[2];
@@ -151,6 +188,18 @@ upward_level_kernel(int level, const int32_t *__restrict__ level_begin,
   }
 }
 
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+upward_level_kernel(int level, const int32_t *__restrict__ level_begin,
+                    const int4 *__restrict__ meta, const int32_t *__restrict__ child,
+                    const double4 *__restrict__ spos, const int32_t *__restrict__ sys_of,
+                    const SysScalars *__restrict__ sys, double4 *com, double *quad, double *oct,
+                    float4 *__restrict__ fq, float4 *__restrict__ fo) {
+  const int lb = level_begin[level], le = level_begin[level + 1];
+  for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x)
+    compute_node<ORDER>(j, meta, child, spos, sys_of, sys, com, quad, oct, fq, fo);
+}
+
 }  // namespace
 
 void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s) {
@@ -158,16 +207,16 @@ void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s) {
   const int grid = grid_for(n / 2 + 1, 128, 148 * 8);
   for (int level = kMaxDepth; level >= 0; --level) {
     if (order >= 8)
-      upward_level_kernel<8><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
+      upward_level_kernel<8><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child, b.spos,
+                                                  b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
     else if (order >= 4)
-      upward_level_kernel<4><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
+      upward_level_kernel<4><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child, b.spos,
+                                                  b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
     else
-      upward_level_kernel<1><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child,
-                                                  b.spos, b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
+      upward_level_kernel<1><<<grid, 128, 0, s>>>(level, b.level_begin, b.cn_meta, b.cn_child, b.spos,
+                                                  b.sys_of, b.ss, b.cn_com, b.cn_quad, b.cn_oct,
                                                   b.cn_fq, b.cn_fo);
   }
 }
