@@ -26,6 +26,7 @@ BH_ERR_NOT_BUILT = 8
 BH_PREC_FP32 = 0
 BH_PREC_FP64 = 1
 BH_PREC_REFERENCE = 2
+BH_PREC_DEHNEN = 3
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTED = [

@@ -39,6 +39,8 @@ struct bh_system {
   int items_pin_cap = 0;
   cudaEvent_t layout_ev = nullptr;
   bool layout_pending = false;
+  // Dehnen's method, allocated on first use
+  bh::DehnenBuffers dehnen;
 };
 
 namespace {
@@ -257,7 +259,7 @@ int check_params(const bh_params *p, int64_t n) {
   if (!(p->eps >= 0.0) || !isfinite(p->eps)) return set_err(BH_ERR_INVALID, "eps must be finite and >= 0");
   if (!isfinite(p->G)) return set_err(BH_ERR_INVALID, "G must be finite");
   if (!(p->amp > 0.0) || !isfinite(p->amp)) return set_err(BH_ERR_INVALID, "amp must be > 0");
-  if (p->precision < 0 || p->precision > 2) return set_err(BH_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (p->precision < 0 || p->precision > 3) return set_err(BH_ERR_INVALID, "precision must be 0, 1, 2 or 3");
   if (p->group_size != 32 && p->group_size != 64) return set_err(BH_ERR_INVALID, "group_size must be 32 or 64");
   if (p->leaf_cap < 1 || p->leaf_cap > 64) return set_err(BH_ERR_INVALID, "leaf_cap must be in 1..64");
   if (p->out_kind != 0 && p->out_kind != 1) return set_err(BH_ERR_INVALID, "out_kind must be 0 or 1");
@@ -326,13 +328,23 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
 }
 
 // the walk of the whole batch, enqueued without host synchronisation
-void enqueue_walk(bh_system *s, const bh_params *p, double *d_out, cudaStream_t st) {
+int enqueue_walk(bh_system *s, const bh_params *p, double *d_out, cudaStream_t st) {
   const bh::WalkParams w = walk_params(p, s->order);
   if (w.count_stats) cudaMemsetAsync(s->b.stats, 0, 4 * sizeof(unsigned long long), st);
+  if (p->precision == BH_PREC_DEHNEN) {
+    switch (bh::run_dehnen(s->n, w, s->b, s->dehnen, d_out, st)) {
+      case 0: return BH_OK;
+      case 1: return set_err(BH_ERR_NOMEM, "Dehnen: device allocation failed");
+      case 2: return set_err(BH_ERR_CUDA, "Dehnen: %s", cudaGetErrorString(cudaGetLastError()));
+      case 3: return set_err(BH_ERR_INTERNAL, "Dehnen: the dual traversal did not close");
+      default: return set_err(BH_ERR_CAPACITY, "Dehnen: more than 2^30 mutual interactions");
+    }
+  }
   if (p->precision == BH_PREC_REFERENCE)
     bh::launch_reference_walk(s->n, w, s->b, d_out, nullptr, 0, nullptr, st);
   else
     bh::launch_walk(s->n, w, s->b, d_out, st);
+  return BH_OK;
 }
 
 int validate_offsets(const int64_t *off, int nsys, int64_t *total) {
@@ -392,7 +404,10 @@ int finish(bh_system *s, cudaStream_t st) {
     if (s->b.sc_host->key_mismatch) {
       bh::launch_adopt_seq_com(s->b, st);
       enqueue_build(s, 1, st);
-      if (s->walked) enqueue_walk(s, &s->walk_p, s->walk_out, st);
+      if (s->walked) {
+        rc = enqueue_walk(s, &s->walk_p, s->walk_out, st);
+        if (rc) return rc;
+      }
       BH_CUDA(cudaGetLastError());
       rc = read_scalars(s, st);
       if (rc) return rc;
@@ -406,7 +421,8 @@ int finish(bh_system *s, cudaStream_t st) {
     rc = ensure_capacity(s, s->n, s->nsys, s->b.n_items);
     if (rc) return rc;
     BH_CUDA(cudaMemsetAsync(&s->b.sc->err, 0, sizeof(int), st));
-    enqueue_walk(s, &s->walk_p, s->walk_out, st);
+    rc = enqueue_walk(s, &s->walk_p, s->walk_out, st);
+    if (rc) return rc;
     BH_CUDA(cudaGetLastError());
     rc = read_scalars(s, st);
     if (rc) return rc;
@@ -514,6 +530,7 @@ int bh_system_destroy(bh_system *s) {
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
   drop_graph(s);
+  bh::free_dehnen(s->dehnen);
   if (!s->fixed_buffers) free_buffers(s->b);
   if (s->items_pin) cudaFreeHost(s->items_pin);
   if (s->layout_ev) cudaEventDestroy(s->layout_ev);
@@ -553,7 +570,8 @@ int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream
   if (p->order > s->order) return set_err(BH_ERR_INVALID, "order %d above the built order %d", p->order, s->order);
   if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
   BH_CUDA(cudaSetDevice(s->device));
-  enqueue_walk(s, p, d_out, (cudaStream_t)stream);
+  rc = enqueue_walk(s, p, d_out, (cudaStream_t)stream);
+  if (rc) return rc;
   BH_CUDA(cudaGetLastError());
   s->walked = 1;
   s->walk_p = *p;
@@ -594,6 +612,8 @@ int bh_system_capture(bh_system *s, const bh_params *p, double *d_out) {
   int rc = check_params(p, s->n);
   if (rc) return rc;
   if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
+  if (p->precision == BH_PREC_DEHNEN)
+    return set_err(BH_ERR_INVALID, "Dehnen's method sizes its lists on the host: no graph capture");
   BH_CUDA(cudaSetDevice(s->device));
   BH_CUDA(cudaDeviceSynchronize());
   drop_graph(s);
@@ -607,7 +627,7 @@ int bh_system_capture(bh_system *s, const bh_params *p, double *d_out) {
   cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     enqueue_build(s, 0, cap);
-    enqueue_walk(s, p, d_out, cap);
+    (void)enqueue_walk(s, p, d_out, cap);
     e = cudaStreamEndCapture(cap, &g);
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&s->graph, g, 0);

@@ -178,6 +178,30 @@ struct WalkParams {
   int count_stats;
   int mac;         // 0 box distance, 1 box distance or every member's own MAC
 };
+// Work buffers of Dehnen's dual-tree method (allocated on first use, grown on
+// demand): entity arrays for nodes and bodies (2n entities), the pair
+// frontier, the mutual pairs and their sorted one-sided terms.
+struct DehnenBuffers {
+  double *rmax = nullptr, *F = nullptr, *H = nullptr, *T = nullptr;
+  int64_t rmax_cap = 0, F_cap = 0, H_cap = 0, T_cap = 0;
+  int2 *front = nullptr, *mut = nullptr;
+  int64_t front_cap = 0, mut_cap = 0;
+  int64_t want_front = 0, want_mut = 0;   // pairs per frontier buffer, mutual pairs
+  uint64_t *keys = nullptr;
+  int32_t *vals = nullptr, *cnt = nullptr, *beg = nullptr, *hist = nullptr, *scan_tmp = nullptr;
+  unsigned long long *counters = nullptr;
+  int64_t keys_cap = 0, vals_cap = 0, cnt_cap = 0, beg_cap = 0, hist_cap = 0, scan_tmp_cap = 0,
+          counters_cap = 0;
+  int64_t pairs = 0;                      // mutual interactions of the last run
+};
+// Dehnen's method over the built batch into out (same layout as the walk).
+// Synchronises the stream once (to size the pair lists).  Returns 0, 1 out of
+// device memory, 2 CUDA error, 3 traversal did not close, 4 pair lists too
+// large.
+int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, double *out,
+               cudaStream_t s);
+void free_dehnen(DehnenBuffers &d);
+
 // Returns the number of warp slots used (for stack sizing).
 void launch_walk(int64_t n, const WalkParams &p, Buffers &b, double *out, cudaStream_t s);
 void launch_reference_walk(int64_t n, const WalkParams &p, Buffers &b, double *out,

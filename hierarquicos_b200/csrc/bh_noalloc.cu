@@ -146,6 +146,10 @@ extern "C" int bh_compute_forces_noalloc(const double *d_m, const double *d_x, c
   }
   if (!d_m || !d_x || !d_y || !d_z || !d_out || !p)
     return bh_report_error(BH_ERR_INVALID, "bh_compute_forces_noalloc: NULL argument");
+  if (p->precision == BH_PREC_DEHNEN)
+    return bh_report_error(BH_ERR_INVALID,
+                           "bh_compute_forces_noalloc: Dehnen's method sizes its pair lists at run "
+                           "time and needs allocated work buffers; use a bh_system");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return bh_report_error(BH_ERR_CUDA, "bh_compute_forces_noalloc: no current CUDA device");

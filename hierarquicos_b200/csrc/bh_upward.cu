@@ -102,7 +102,12 @@ __device__ void compute_node(int j, const int4 *__restrict__ meta, const int32_t
       cy = cy + p.w * p.y;
       cz = cz + p.w * p.z;
     }
-    cx = cx / M; cy = cy / M; cz = cz / M;
+    if (M == 0.0) {  // massless node: a finite centre (it only enters sums times 0)
+      const double4 p = spos[mt.x];
+      cx = p.x; cy = p.y; cz = p.z;
+    } else {
+      cx = cx / M; cy = cy / M; cz = cz / M;
+    }
     com[j] = make_double4(cx, cy, cz, M);
     if constexpr (ORDER < 4) {
       return;
@@ -142,7 +147,11 @@ __device__ void compute_node(int j, const int4 *__restrict__ meta, const int32_t
         cz = cz + cd[c].w * cd[c].z;
       }
     }
-    cx = cx / M; cy = cy / M; cz = cz / M;
+    if (M == 0.0) {  // massless node: a finite centre (it only enters sums times 0)
+      cx = cd[0].x; cy = cd[0].y; cz = cd[0].z;
+    } else {
+      cx = cx / M; cy = cy / M; cz = cz / M;
+    }
     com[j] = make_double4(cx, cy, cz, M);
     if constexpr (ORDER < 4) {
       return;

@@ -19,7 +19,7 @@ import torch
 from . import _lib
 from ._lib import BHParams, check, default_params, lib
 
-ORDER_OF_METHOD = {10: 1, 11: 4, 12: 8, 30: 1, 31: 4, 32: 8}
+ORDER_OF_METHOD = {10: 1, 11: 4, 12: 8, 20: 1, 21: 4, 22: 8, 30: 1, 31: 4, 32: 8}
 
 
 def _dptr(t: torch.Tensor) -> int:
@@ -284,12 +284,14 @@ class MortonTree:
 
 
 class Octree:
-    """Mirror of OctreeType's Barnes-Hut part (octree_default.f90:90-170).
+    """Mirror of OctreeType's force methods (octree_default.f90:90-170).
 
     ``pre_init(m, method, group_size=64)`` with method 10/11/12 (classic BH,
-    monopole/quadrupole/octupole) or 30/31/32 (grouped BH); ``init(x, y, z)``;
-    ``forces_groups(theta2, G, eps2)`` returns forces (3,N).  Methods 10-12 run
-    the per-target reference walk, 30-32 the warp-cooperative group walk."""
+    monopole/quadrupole/octupole), 20/21/22 (Dehnen's dual-tree method) or
+    30/31/32 (grouped BH); ``init(x, y, z)``; ``forces_groups(theta2, G, eps2)``
+    (and ``dehnen_eval(theta2, eps2, G)`` for 20-22) returns forces (3,N).
+    Methods 10-12 run the per-target reference walk, 20-22 the device dual
+    traversal, 30-32 the warp-cooperative group walk."""
 
     def __init__(self):
         self.sys = None
@@ -297,7 +299,7 @@ class Octree:
     def pre_init(self, m, method: int = 31, collide: bool = False, radii=None,
                  group_size: int = 64):
         if method not in ORDER_OF_METHOD:
-            raise ValueError(f"method {method} not identified (10-12, 30-32)")
+            raise ValueError(f"method {method} not identified (10-12, 20-22, 30-32)")
         self.m = np.ascontiguousarray(m, np.float64)
         self.N = self.m.size
         self.method = method
@@ -314,8 +316,15 @@ class Octree:
         self.sys.sync()
         return self
 
+    def dehnen_eval(self, theta2: float, potsoft2: float, G: float, forces=None, nt_par=None):
+        """octree_default.f90:1676-1712 (dehnen_eval): argument order as there."""
+        if self.method not in (20, 21, 22):
+            raise ValueError("dehnen_eval needs method 20, 21 or 22")
+        return self.forces_groups(theta2, G, potsoft2, forces)
+
     def forces_groups(self, theta2: float, G: float, eps2: float, forces=None, nt=None):
-        prec = _lib.BH_PREC_REFERENCE if self.method < 30 else _lib.BH_PREC_FP32
+        prec = {1: _lib.BH_PREC_REFERENCE, 2: _lib.BH_PREC_DEHNEN, 3: _lib.BH_PREC_FP32}[
+            self.method // 10]
         p = default_params(order=self.multipole, group_size=self.group_size, precision=prec,
                            theta=float(np.sqrt(theta2)), G=G, eps=float(np.sqrt(eps2)))
         out = self.sys.walk(p)

@@ -38,6 +38,9 @@ extern "C" {
 #define BH_PREC_FP32 0       /* warp-cooperative group walk, FP32, Kahan-compensated */
 #define BH_PREC_FP64 1       /* the same group walk in FP64                          */
 #define BH_PREC_REFERENCE 2  /* per-target FP64 walk with the reference's MAC        */
+#define BH_PREC_DEHNEN 3     /* Dehnen's dual-tree method in FP64 (octree_default.f90
+                                :1095-1712, methods 20/21/22); the call synchronises
+                                its stream once and cannot be captured in a graph    */
 
 typedef struct bh_params {
     double theta;     /* opening angle, unsquared                                 */

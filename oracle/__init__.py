@@ -59,6 +59,8 @@ def lib():
                                         _dp, C.c_int]
         L.orc_morton_forces_targets.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                                 C.c_int, C.c_int64, _i64p, _dp, C.c_void_p, C.c_int]
+        L.orc_morton_dehnen.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        _dp, C.POINTER(C.c_int64)]
         L.orc_octree_create.argtypes = [C.c_int64, _dp, C.c_int, C.c_int, C.c_int64,
                                         C.POINTER(C.c_void_p)]
         L.orc_octree_init.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -178,6 +180,16 @@ class MortonTree:
         _check(lib().orc_morton_forces(self._h, G, eps2, theta2, int(mult), out, nthreads))
         return out.reshape(3, self.n).T
 
+    def dehnen(self, G: float, eps2: float, theta2: float, mult: int = 4, pairs: bool = False):
+        """Dehnen's dual-tree method (octree_default.f90:1095-1712) over this
+        Morton tree: forces (N,3) in original order; with pairs=True also the
+        number of mutual interactions."""
+        out = np.empty(3 * self.n)
+        npairs = C.c_int64(0)
+        _check(lib().orc_morton_dehnen(self._h, G, eps2, theta2, int(mult), out, C.byref(npairs)))
+        f = out.reshape(3, self.n).T
+        return (f, npairs.value) if pairs else f
+
     def forces_targets(self, targets, G, eps2, theta2, mult=True, nthreads: int = 0):
         """(forces (k,3), counts (k,2) = body-body, cell) for ORIGINAL indices."""
         t = np.ascontiguousarray(targets, dtype=np.int64)
@@ -189,7 +201,10 @@ class MortonTree:
 
 
 class Octree:
-    """OctreeType (octree_default.f90:90-170): pre_init + init + forces."""
+    """OctreeType (octree_default.f90:90-170): pre_init + init + forces.
+    method 10-12 classic BH, 20-22 Dehnen's dual-tree method (forces() runs
+    dehnen_eval), 30-32 grouped BH; the last digit picks monopole, quadrupole
+    or octupole."""
 
     def __init__(self, m, method: int = 11, group_size: int = 64, max_nodes: int = 0):
         m = _f64(m)

@@ -609,7 +609,8 @@ void orc_octree_free(orc_octree *t) {
 }
 
 /* octree_default.f90:178-282 (pre_init).  method: 10/11/12 classic BH with
- * monopole/quadrupole/octupole, 30/31/32 grouped BH.  max_nodes == 0 keeps the
+ * monopole/quadrupole/octupole, 20/21/22 Dehnen's dual-tree method, 30/31/32
+ * grouped BH.  max_nodes == 0 keeps the
  * reference's node budget (3N for N >= 1000, else 10N, :219-223); a larger
  * budget may be passed for strongly clustered inputs where the reference would
  * stop with "INSUFFICIENT NUMBER OF NODES". */
@@ -622,7 +623,10 @@ int orc_octree_create(int64_t n, const double *m, int method, int group_size, in
     case 10: case 30: mp = 1; break;
     case 11: case 31: mp = 4; break;
     case 12: case 32: mp = 8; break;
-    default: return fail(ORC_EINVAL, "octree: method must be 10-12 or 30-32");
+    case 20: mp = 1; break;
+    case 21: mp = 4; break;
+    case 22: mp = 8; break;
+    default: return fail(ORC_EINVAL, "octree: method must be 10-12, 20-22 or 30-32");
     }
     orc_octree *t = (orc_octree *)calloc(1, sizeof(orc_octree));
     if (!t) return fail(ORC_ENOMEM, "octree: out of memory");
@@ -1136,9 +1140,12 @@ static void group_forces(const orc_octree *t, int64_t gi, double theta2, double 
 /* Forces for all particles, ORIGINAL order, SoA out.  Methods 10-12 follow
  * test_forces.f90:201-211 (per-particle loop), 30-32 follow forces_groups
  * (octree_default.f90:1811-1831). */
+static int octree_dehnen(const orc_octree *t, double theta2, double G, double eps2, double *out);
+
 int orc_octree_forces(const orc_octree *t, double theta2, double G, double eps2, double *out,
                       int nthreads) {
     int64_t n = t->n;
+    if (t->method >= 20 && t->method < 30) return octree_dehnen(t, theta2, G, eps2, out);
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #endif
@@ -1183,7 +1190,7 @@ int orc_octree_forces(const orc_octree *t, double theta2, double G, double eps2,
 int orc_octree_forces_targets(const orc_octree *t, double theta2, double G, double eps2,
                               int64_t nt, const int64_t *targets, double *out, int64_t *counts,
                               int nthreads) {
-    if (t->method >= 30) return fail(ORC_EINVAL, "targets: per-particle methods only");
+    if (t->method >= 20) return fail(ORC_EINVAL, "targets: per-particle methods only");
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel num_threads(nthreads)
@@ -1260,4 +1267,371 @@ int orc_num_threads(void) {
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* Dehnen's dual-tree method, fortran/octree_default.f90:1095-1712 (methods
+ * 20/21/22): evaluate_rmax (:1095-1131), mutual_interaction_walk_sequential
+ * (:1133-1247), the mutual interactions (monopole :1425-1445; quadrupole
+ * :1447-1558, with the octupole torque term for multipole 8) and dehnen_forces
+ * (:1560-1673, the downward pass).  It runs over a generic view of a tree --
+ * entities in parent-before-child order with CSR child lists -- so the same
+ * code serves the insertion tree (the reference's own) and the Morton tree
+ * (whose topology the device build reproduces).  Forces are G m a, SoA
+ * (x block, y block, z block) in the particles' output order. */
+
+typedef struct {
+    int64_t ne;
+    int64_t *cbeg;      /* ne + 1 */
+    int32_t *clist;
+    int32_t *leaf;      /* 1: a particle leaf (ns_type == 1) */
+    int64_t *particle;  /* output index of a leaf's particle, -1 none */
+    double *mass, *cx, *cy, *cz;
+    double *quad;       /* 6 per entity (multipole >= 4), raw moments about the COM */
+    double *oct;        /* 14 per entity (multipole >= 8), octree_default layout */
+} dtree;
+
+static void dtree_free(dtree *t) {
+    free(t->cbeg); free(t->clist); free(t->leaf); free(t->particle);
+    free(t->mass); free(t->quad); free(t->oct);
+}
+
+static int dtree_alloc(dtree *t, int64_t ne, int64_t nlinks) {
+    memset(t, 0, sizeof *t);
+    t->ne = ne;
+    t->cbeg = (int64_t *)calloc((size_t)ne + 1, sizeof(int64_t));
+    t->clist = (int32_t *)malloc((size_t)(nlinks > 0 ? nlinks : 1) * sizeof(int32_t));
+    t->leaf = (int32_t *)calloc((size_t)ne, sizeof(int32_t));
+    t->particle = (int64_t *)malloc((size_t)ne * sizeof(int64_t));
+    t->mass = (double *)calloc((size_t)ne * 4, sizeof(double));
+    t->quad = (double *)calloc((size_t)ne * 6, sizeof(double));
+    t->oct = (double *)calloc((size_t)ne * 14, sizeof(double));
+    if (!t->cbeg || !t->clist || !t->leaf || !t->particle || !t->mass || !t->quad || !t->oct) {
+        dtree_free(t);
+        return fail(ORC_ENOMEM, "dehnen: out of memory");
+    }
+    t->cx = t->mass + ne; t->cy = t->cx + ne; t->cz = t->cy + ne;
+    return ORC_OK;
+}
+
+/* ind_oct of octree_default.f90:233-241, 0-based: component of O_jkl */
+static const int IND_OCT[3][3][3] = {
+    {{0, 3, 6}, {3, 1, 9}, {6, 9, 2}},
+    {{3, 1, 9}, {1, 4, 7}, {9, 7, 5}},
+    {{6, 9, 2}, {9, 7, 5}, {2, 5, 8}}};
+
+/* :1095-1131 */
+static void dehnen_rmax(const dtree *t, double *rmax) {
+    for (int64_t e = t->ne - 1; e >= 0; --e) {
+        rmax[e] = 0.0;
+        if (t->leaf[e]) continue;
+        double r = 0.0;
+        for (int64_t k = t->cbeg[e]; k < t->cbeg[e + 1]; ++k) {
+            int64_t c = t->clist[k];
+            if (t->mass[c] == 0.0) continue;
+            double dx = t->cx[c] - t->cx[e];
+            double dy = t->cy[c] - t->cy[e];
+            double dz = t->cz[c] - t->cz[e];
+            double dist = sqrt(dx * dx + dy * dy + dz * dz);
+            double v = dist + rmax[c];
+            if (v > r) r = v;
+        }
+        rmax[e] = r;
+    }
+}
+
+/* :1425-1445 (monopole) and :1447-1558 (quadrupole, octupole torque term),
+ * accumulated into both nodes as :1200-1221 does. */
+static void dehnen_mutual(const dtree *t, int mult, int64_t a, int64_t b, double G, double eps2,
+                          double *F, double *H, double *T) {
+    const double Ma = t->mass[a], Mb = t->mass[b];
+    if (mult == 1) {
+        double dx = t->cx[b] - t->cx[a];
+        double dy = t->cy[b] - t->cy[a];
+        double dz = t->cz[b] - t->cz[a];
+        double dist2 = dx * dx + dy * dy + dz * dz;
+        double rinv3 = 1.0 / pow(dist2 + eps2, 1.5);
+        double factor = G * rinv3;
+        double f[3] = {factor * dx, factor * dy, factor * dz};
+        for (int k = 0; k < 3; ++k) {
+            F[3 * a + k] = F[3 * a + k] + Mb * f[k];
+            F[3 * b + k] = F[3 * b + k] - Ma * f[k];
+        }
+        return;
+    }
+    double dx = t->cx[a] - t->cx[b];
+    double dy = t->cy[a] - t->cy[b];
+    double dz = t->cz[a] - t->cz[b];
+    double r2 = dx * dx + dy * dy + dz * dz + eps2;
+    double rinv3 = 1.0 / pow(r2, 1.5);
+    double rinv5 = 1.0 / pow(r2, 2.5);
+    double rinv7 = 1.0 / pow(r2, 3.5);
+    double D1[3], D2[6], D3[10];
+    D1[0] = -G * dx * rinv3;
+    D1[1] = -G * dy * rinv3;
+    D1[2] = -G * dz * rinv3;
+    D2[0] = G * (3.0 * dx * dx * rinv5 - rinv3);
+    D2[1] = G * (3.0 * dy * dy * rinv5 - rinv3);
+    D2[2] = G * (3.0 * dz * dz * rinv5 - rinv3);
+    D2[3] = G * 3.0 * dx * dy * rinv5;
+    D2[4] = G * 3.0 * dx * dz * rinv5;
+    D2[5] = G * 3.0 * dy * dz * rinv5;
+    D3[0] = G * (-15.0 * dx * dx * dx * rinv7 + 9.0 * dx * rinv5);
+    D3[1] = G * (-15.0 * dx * dx * dy * rinv7 + 3.0 * dy * rinv5);
+    D3[2] = G * (-15.0 * dx * dx * dz * rinv7 + 3.0 * dz * rinv5);
+    D3[3] = G * (-15.0 * dx * dy * dy * rinv7 + 3.0 * dx * rinv5);
+    D3[4] = G * (-15.0 * dx * dy * dz * rinv7);
+    D3[5] = G * (-15.0 * dx * dz * dz * rinv7 + 3.0 * dx * rinv5);
+    D3[6] = G * (-15.0 * dy * dy * dy * rinv7 + 9.0 * dy * rinv5);
+    D3[7] = G * (-15.0 * dy * dy * dz * rinv7 + 3.0 * dz * rinv5);
+    D3[8] = G * (-15.0 * dy * dz * dz * rinv7 + 3.0 * dy * rinv5);
+    D3[9] = G * (-15.0 * dz * dz * dz * rinv7 + 9.0 * dz * rinv5);
+    double Qa[6], Qb[6];
+    for (int k = 0; k < 6; ++k) { Qa[k] = t->quad[6 * a + k] / Ma; Qb[k] = t->quad[6 * b + k] / Mb; }
+    double CQa[3], CQb[3];
+    CQa[0] = Qa[0] * D3[0] + 2.0 * Qa[3] * D3[1] + 2.0 * Qa[4] * D3[2] + Qa[1] * D3[3] +
+             2.0 * Qa[5] * D3[4] + Qa[2] * D3[5];
+    CQb[0] = Qb[0] * D3[0] + 2.0 * Qb[3] * D3[1] + 2.0 * Qb[4] * D3[2] + Qb[1] * D3[3] +
+             2.0 * Qb[5] * D3[4] + Qb[2] * D3[5];
+    CQa[1] = Qa[0] * D3[1] + 2.0 * Qa[3] * D3[3] + 2.0 * Qa[4] * D3[4] + Qa[1] * D3[6] +
+             2.0 * Qa[5] * D3[7] + Qa[2] * D3[8];
+    CQb[1] = Qb[0] * D3[1] + 2.0 * Qb[3] * D3[3] + 2.0 * Qb[4] * D3[4] + Qb[1] * D3[6] +
+             2.0 * Qb[5] * D3[7] + Qb[2] * D3[8];
+    CQa[2] = Qa[0] * D3[2] + 2.0 * Qa[3] * D3[4] + 2.0 * Qa[4] * D3[5] + Qa[1] * D3[7] +
+             2.0 * Qa[5] * D3[8] + Qa[2] * D3[9];
+    CQb[2] = Qb[0] * D3[2] + 2.0 * Qb[3] * D3[4] + 2.0 * Qb[4] * D3[5] + Qb[1] * D3[7] +
+             2.0 * Qb[5] * D3[8] + Qb[2] * D3[9];
+    double fa[3], fb[3], fc[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < 3; ++k) {
+        fa[k] = Mb * (D1[k] + 0.5 * CQb[k]);
+        fb[k] = -Ma * (D1[k] + 0.5 * CQa[k]);
+    }
+    if (mult >= 8) {
+        double R[3] = {dx, dy, dz}, ci[3] = {0, 0, 0}, CRR[3] = {0, 0, 0};
+        for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k)
+                for (int l = 0; l < 3; ++l) {
+                    double Cjkl = Mb * t->oct[14 * a + IND_OCT[j][k][l]] -
+                                  Ma * t->oct[14 * b + IND_OCT[j][k][l]];
+                    if (k == l) ci[j] = ci[j] + Cjkl;
+                    CRR[j] = CRR[j] + Cjkl * R[k] * R[l];
+                }
+        for (int k = 0; k < 3; ++k)
+            fc[k] = 0.5 * (3.0 * G * rinv5 * ci[k] - 15.0 * G * rinv7 * CRR[k]);
+    }
+    for (int k = 0; k < 3; ++k) {
+        F[3 * a + k] = F[3 * a + k] + fa[k] + fc[k] / Ma;
+        F[3 * b + k] = F[3 * b + k] + fb[k] - fc[k] / Mb;
+    }
+    for (int k = 0; k < 6; ++k) {
+        H[6 * a + k] = H[6 * a + k] + Mb * D2[k];
+        H[6 * b + k] = H[6 * b + k] + Ma * D2[k];
+    }
+    for (int k = 0; k < 10; ++k) {
+        T[10 * a + k] = T[10 * a + k] + Mb * D3[k];
+        T[10 * b + k] = T[10 * b + k] - Ma * D3[k];
+    }
+}
+
+/* The whole method on entity 0 as the root.  *pairs (optional) returns the
+ * number of mutual interactions. */
+static int dehnen_run(const dtree *t, int mult, double theta2, double G, double eps2, int64_t n,
+                      double *out, int64_t *pairs) {
+    const int64_t ne = t->ne;
+    double *rmax = (double *)malloc((size_t)ne * sizeof(double));
+    double *F = (double *)calloc((size_t)ne * 3, sizeof(double));
+    double *H = (double *)calloc((size_t)ne * 6, sizeof(double));
+    double *T = (double *)calloc((size_t)ne * 10, sizeof(double));
+    int64_t cap = 36 * ne + 64, top = 0, np = 0;
+    int64_t *st = (int64_t *)malloc((size_t)cap * 2 * sizeof(int64_t));
+    if (!rmax || !F || !H || !T || !st) {
+        free(rmax); free(F); free(H); free(T); free(st);
+        return fail(ORC_ENOMEM, "dehnen: out of memory");
+    }
+    for (int64_t i = 0; i < 3 * n; ++i) out[i] = 0.0;
+    dehnen_rmax(t, rmax);
+#define PUSH(A, B)                                                                  \
+    do {                                                                            \
+        if (top == cap) {                                                           \
+            cap *= 2;                                                               \
+            int64_t *ns = (int64_t *)realloc(st, (size_t)cap * 2 * sizeof(int64_t)); \
+            if (!ns) { free(st); st = NULL; goto oom; }                              \
+            st = ns;                                                                \
+        }                                                                           \
+        st[2 * top] = (A); st[2 * top + 1] = (B); ++top;                            \
+    } while (0)
+    PUSH(0, 0);
+    while (top > 0) {
+        --top;
+        const int64_t a = st[2 * top], b = st[2 * top + 1];
+        if (t->mass[a] == 0.0) continue;
+        if (t->mass[b] == 0.0) continue;
+        if (a == b) {
+            if (t->leaf[a]) continue;
+            for (int64_t i = t->cbeg[a]; i < t->cbeg[a + 1]; ++i)
+                for (int64_t j = i; j < t->cbeg[a + 1]; ++j) PUSH(t->clist[i], t->clist[j]);
+            continue;
+        }
+        double dx = t->cx[a] - t->cx[b];
+        double dy = t->cy[a] - t->cy[b];
+        double dz = t->cz[a] - t->cz[b];
+        double dist2 = dx * dx + dy * dy + dz * dz;
+        double rs = rmax[a] + rmax[b];
+        double rsum2 = rs * rs;
+        if (rsum2 <= theta2 * dist2) {
+            dehnen_mutual(t, mult, a, b, G, eps2, F, H, T);
+            ++np;
+            continue;
+        }
+        if (rmax[a] >= rmax[b]) {
+            for (int64_t i = t->cbeg[a]; i < t->cbeg[a + 1]; ++i) PUSH(t->clist[i], b);
+        } else {
+            for (int64_t i = t->cbeg[b]; i < t->cbeg[b + 1]; ++i) PUSH(a, t->clist[i]);
+        }
+    }
+#undef PUSH
+    /* :1560-1673 downward pass */
+    for (int64_t e = 0; e < ne; ++e) {
+        if (t->leaf[e]) continue;
+        const double *h = H + 6 * e, *tt = T + 10 * e;
+        for (int64_t k = t->cbeg[e]; k < t->cbeg[e + 1]; ++k) {
+            const int64_t c = t->clist[k];
+            if (t->mass[c] == 0.0) continue;
+            double fch[3];
+            for (int q = 0; q < 3; ++q) fch[q] = F[3 * c + q] + F[3 * e + q];
+            if (mult >= 4) {
+                double dx = t->cx[c] - t->cx[e];
+                double dy = t->cy[c] - t->cy[e];
+                double dz = t->cz[c] - t->cz[e];
+                const double hxx = h[0], hyy = h[1], hzz = h[2], hxy = h[3], hxz = h[4], hyz = h[5];
+                const double txxx = tt[0], txxy = tt[1], txxz = tt[2], txyy = tt[3], txyz = tt[4],
+                             txzz = tt[5], tyyy = tt[6], tyyz = tt[7], tyzz = tt[8], tzzz = tt[9];
+                fch[0] = fch[0] + hxx * dx + hxy * dy + hxz * dz + txxy * dx * dy + txxz * dx * dz +
+                         txyz * dy * dz + 0.5 * (txxx * dx * dx + txyy * dy * dy + txzz * dz * dz);
+                fch[1] = fch[1] + hxy * dx + hyy * dy + hyz * dz + txyy * dx * dy + txyz * dx * dz +
+                         tyyz * dy * dz + 0.5 * (txxy * dx * dx + tyyy * dy * dy + tyzz * dz * dz);
+                fch[2] = fch[2] + hxz * dx + hyz * dy + hzz * dz + txyz * dx * dy + txzz * dx * dz +
+                         tyzz * dy * dz + 0.5 * (txxz * dx * dx + tyyz * dy * dy + tzzz * dz * dz);
+                if (!t->leaf[c]) {
+                    double *hc = H + 6 * c;
+                    hc[0] = hc[0] + hxx + txxx * dx + txxy * dy + txxz * dz;
+                    hc[1] = hc[1] + hyy + txyy * dx + tyyy * dy + tyyz * dz;
+                    hc[2] = hc[2] + hzz + txzz * dx + tyzz * dy + tzzz * dz;
+                    hc[3] = hc[3] + hxy + txxy * dx + txyy * dy + txyz * dz;
+                    hc[4] = hc[4] + hxz + txxz * dx + txyz * dy + txzz * dz;
+                    hc[5] = hc[5] + hyz + txyz * dx + tyyz * dy + tyzz * dz;
+                }
+                for (int q = 0; q < 10; ++q) T[10 * c + q] = T[10 * c + q] + tt[q];
+            }
+            for (int q = 0; q < 3; ++q) F[3 * c + q] = fch[q];
+            if (t->leaf[c]) {
+                const int64_t p = t->particle[c];
+                if (p < 0) continue;
+                for (int q = 0; q < 3; ++q) out[q * n + p] = t->mass[c] * F[3 * c + q];
+            }
+        }
+    }
+    if (pairs) *pairs = np;
+    free(rmax); free(F); free(H); free(T); free(st);
+    return ORC_OK;
+oom:
+    free(rmax); free(F); free(H); free(T);
+    return fail(ORC_ENOMEM, "dehnen: out of memory for the pair stack");
+}
+
+/* Insertion tree (octree_default) as a generic tree. */
+static int octree_dehnen(const orc_octree *t, double theta2, double G, double eps2, double *out) {
+    dtree d;
+    int64_t links = 0;
+    for (int64_t e = 0; e < t->nnodes; ++e)
+        for (int c = 0; c < 8; ++c) links += t->child[8 * e + c] != -1;
+    int rc = dtree_alloc(&d, t->nnodes, links);
+    if (rc) return rc;
+    int64_t k = 0;
+    for (int64_t e = 0; e < t->nnodes; ++e) {
+        d.cbeg[e] = k;
+        for (int c = 0; c < 8; ++c)
+            if (t->child[8 * e + c] != -1) d.clist[k++] = t->child[8 * e + c];
+        d.leaf[e] = t->type[e] == 1;
+        d.particle[e] = t->type[e] == 1 ? t->particle[e] : -1;
+        d.mass[e] = t->mass[e]; d.cx[e] = t->qx[e]; d.cy[e] = t->qy[e]; d.cz[e] = t->qz[e];
+        if (t->multipole >= 4) memcpy(d.quad + 6 * e, t->quad + 6 * e, 6 * sizeof(double));
+        if (t->multipole >= 8) memcpy(d.oct + 14 * e, t->oct + 14 * e, 14 * sizeof(double));
+    }
+    d.cbeg[t->nnodes] = k;
+    rc = dehnen_run(&d, t->multipole, theta2, G, eps2, t->n, out, NULL);
+    dtree_free(&d);
+    return rc;
+}
+
+/* Raw second and third moments of sorted particles [first, last] about c,
+ * with the summary sums of octree_default.f90:875-880. */
+static void direct_moments(const orc_morton *t, int64_t first, int64_t last, const double c[3],
+                           double *Q, double *O) {
+    for (int k = 0; k < 6; ++k) Q[k] = 0.0;
+    for (int k = 0; k < 14; ++k) O[k] = 0.0;
+    for (int64_t p = first; p <= last; ++p) {
+        const double pm = t->ms[p];
+        const double dx = t->qx[p] - c[0], dy = t->qy[p] - c[1], dz = t->qz[p] - c[2];
+        Q[0] += pm * dx * dx; Q[1] += pm * dy * dy; Q[2] += pm * dz * dz;
+        Q[3] += pm * dx * dy; Q[4] += pm * dx * dz; Q[5] += pm * dy * dz;
+        O[0] += pm * dx * dx * dx; O[1] += pm * dx * dy * dy; O[2] += pm * dx * dz * dz;
+        O[3] += pm * dy * dx * dx; O[4] += pm * dy * dy * dy; O[5] += pm * dy * dz * dz;
+        O[6] += pm * dz * dx * dx; O[7] += pm * dz * dy * dy; O[8] += pm * dz * dz * dz;
+        O[9] += pm * dx * dy * dz;
+    }
+    double s = 0.0;
+    for (int k = 0; k < 10; ++k) s += O[k];
+    O[10] = s;
+    O[11] = O[0] + O[1] + O[2];
+    O[12] = O[3] + O[4] + O[5];
+    O[13] = O[6] + O[7] + O[8];
+}
+
+/* Morton tree (morton_octree.f90) as a generic tree: a node of one particle
+ * is a particle leaf at its centre of mass; a depth-L node of several bodies
+ * (identical keys) gets one particle leaf per body, appended after the nodes;
+ * moments are summed directly over each node's bodies.  mult 1, 4 or 8. */
+int orc_morton_dehnen(const orc_morton *t, double G, double eps2, double theta2, int mult,
+                      double *out, int64_t *pairs) {
+    if (mult != 1 && mult != 4 && mult != 8) return fail(ORC_EINVAL, "dehnen: mult must be 1, 4 or 8");
+    const int64_t nn = t->nnodes;
+    int64_t extra = 0, links = 0;
+    for (int64_t e = 0; e < nn; ++e) {
+        if (t->first[e] == t->last[e]) continue;
+        if (t->nchild[e] == 0) { extra += t->last[e] - t->first[e] + 1; links += t->last[e] - t->first[e] + 1; }
+        else links += t->nchild[e];
+    }
+    dtree d;
+    int rc = dtree_alloc(&d, nn + extra, links);
+    if (rc) return rc;
+    int64_t k = 0, nx = nn;
+    for (int64_t e = 0; e < nn; ++e) {
+        d.cbeg[e] = k;
+        d.mass[e] = t->nmass[e];
+        d.cx[e] = t->qcm[3 * e]; d.cy[e] = t->qcm[3 * e + 1]; d.cz[e] = t->qcm[3 * e + 2];
+        d.particle[e] = -1;
+        if (t->first[e] == t->last[e]) {
+            d.leaf[e] = 1;
+            d.particle[e] = t->perm[t->first[e]];
+            continue;
+        }
+        direct_moments(t, t->first[e], t->last[e], t->qcm + 3 * e, d.quad + 6 * e, d.oct + 14 * e);
+        if (t->nchild[e] == 0) {
+            for (int64_t p = t->first[e]; p <= t->last[e]; ++p) {
+                d.clist[k++] = (int32_t)nx;
+                d.leaf[nx] = 1;
+                d.particle[nx] = t->perm[p];
+                d.mass[nx] = t->ms[p];
+                d.cx[nx] = t->qx[p]; d.cy[nx] = t->qy[p]; d.cz[nx] = t->qz[p];
+                ++nx;
+            }
+        } else {
+            for (int c = 0; c < t->nchild[e]; ++c) d.clist[k++] = t->child[8 * e + c];
+        }
+    }
+    for (int64_t e = nn; e <= nn + extra; ++e) d.cbeg[e] = k;
+    rc = dehnen_run(&d, mult, theta2, G, eps2, t->n, out, pairs);
+    dtree_free(&d);
+    return rc;
 }

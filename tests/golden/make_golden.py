@@ -4,7 +4,10 @@
    in benchmarks/forces_time_and_error/out/aarseth/test_{monopole,quadrupole,
    octupole}.txt (produced by benchmarks/forces_time_and_error/
    forces_time_and_error.f90:66-111 and :204-308: Plummer spheres, size 10,
-   b = 0.58, eps = 0, N = 1024 and 4096, 21 draws per N, methods 10/11/12).
+   b = 0.58, eps = 0, N = 1024 and 4096, 21 draws per N, methods 10/11/12),
+   and for Dehnen's method in benchmarks/dehnen/out/direct_vs_bh_vs_dehnen/
+   dehnen_{monopole,quadrupole}.txt (benchmarks/dehnen/forces_dehnen.f90:
+   13-153, the same spheres, N = 5000 and 10000, 6 draws, methods 20/21).
    For each (order, N, theta) the median and the 10th/90th percentiles of the
    recorded normalised RMS error are stored.  Needs the reference checkout
    (REFERENCE_ROOT, default /root/reference); run only where it exists.
@@ -45,6 +48,20 @@ def recorded_errors():
                     order=order, n=int(n), theta=float(round(th, 1)), count=int(e.size),
                     median=float(np.median(e)), p10=float(np.percentile(e, 10)),
                     p90=float(np.percentile(e, 90)))
+    # Dehnen's method (methods 20/21): benchmarks/dehnen/forces_dehnen.f90:13-153
+    # (Plummer, size 10, b = 0.58, eps = 0, 6 draws per N), keys "dehnen<order>/N/theta"
+    base = os.path.join(REFERENCE_ROOT, "benchmarks", "dehnen", "out", "direct_vs_bh_vs_dehnen")
+    for order, name in ((1, "dehnen_monopole"), (4, "dehnen_quadrupole")):
+        rows = np.loadtxt(os.path.join(base, f"{name}.txt"))
+        rows = rows[rows[:, 1] > 0]
+        for n in (5000, 10000):
+            for th in np.unique(rows[:, 1]):
+                sel = rows[(rows[:, 0] == n) & (rows[:, 1] == th)]
+                e, e2 = sel[:, 4], sel[:, 6]
+                out[f"dehnen{order}/{n}/{th:.1f}"] = dict(
+                    order=order, n=int(n), theta=float(round(th, 1)), count=int(e.size),
+                    median=float(np.median(e)), p10=float(np.percentile(e, 10)),
+                    p90=float(np.percentile(e, 90)), median_rel_l2=float(np.median(e2)))
     with open(os.path.join(HERE, "recorded_errors.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     print("wrote recorded_errors.json", len(out))
@@ -71,10 +88,11 @@ def oracle_small():
     fo = oracle.Octree(m, 12).init(x, y, z).forces(0.5 ** 2, 1.0, 0.01 ** 2)
     fg = oracle.Octree(m, 31).init(x, y, z).forces(0.5 ** 2, 1.0, 0.01 ** 2)
     fd = oracle.direct_forces(m, x, y, z, 1.0, 0.01 ** 2)
+    fdh = oracle.Octree(m, 21).init(x, y, z).forces(0.5 ** 2, 1.0, 0.01 ** 2)
     np.savez_compressed(os.path.join(HERE, "oracle_small.npz"), m10=m10, x10=x10, y10=y10,
                         z10=z10, L10=t10.L, keys10=k10, perm10=p10, forces10=f10, m=m, x=x, y=y,
                         z=z, keys=k, perm=p, forces_morton_quad=f, forces_octupole=fo,
-                        forces_grouped_quad=fg, forces_direct=fd)
+                        forces_grouped_quad=fg, forces_direct=fd, forces_dehnen_quad=fdh)
     print("wrote oracle_small.npz")
 
 

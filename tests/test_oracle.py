@@ -105,6 +105,8 @@ def test_oracle_reproduces_golden_vectors(oracle_mod):
     assert np.array_equal(fo, g["forces_octupole"])
     fd = oracle_mod.direct_forces(g["m"], g["x"], g["y"], g["z"], 1.0, 1e-4)
     assert np.array_equal(fd, g["forces_direct"])
+    fdh = oracle_mod.Octree(g["m"], 21).init(g["x"], g["y"], g["z"]).forces(0.25, 1.0, 1e-4)
+    assert np.array_equal(fdh, g["forces_dehnen_quad"])
 
 
 def test_keys_fma_modes_differ_only_near_cell_edges(oracle_mod):
@@ -114,3 +116,57 @@ def test_keys_fma_modes_differ_only_near_cell_edges(oracle_mod):
     k0, *_ = oracle_mod.morton_keys(m, *xyz(q), 21, 1.2, 0)
     k1, *_ = oracle_mod.morton_keys(m, *xyz(q), 21, 1.2, 1)
     assert np.mean(k0 == k1) > 0.999
+
+
+@pytest.mark.parametrize("order,method", [(1, 20), (4, 21)])
+def test_oracle_dehnen_matches_recorded_error_statistics(oracle_mod, recorded, order, method):
+    """Statistical pin of Dehnen's method: benchmarks/dehnen/forces_dehnen.f90
+    recorded the normalised RMS error of methods 20/21 (Plummer, size 10,
+    b = 0.58, eps = 0, N = 5000, 6 draws); the oracle's median over 5 seeded
+    draws must fall inside [0.6 x p10, 1.6 x p90] of the recorded draws."""
+    from hierarquicos_b200.initial_values import generate_initial_values
+
+    n = 5000
+    thetas = [0.2, 0.6, 1.0]
+    errs = {th: [] for th in thetas}
+    for seed in range(5):
+        m, q, _ = generate_initial_values(n, 10.0, 0.0, True, False, "plummer", (1.0, 0.58),
+                                          seed=100 + seed, velocities=False)
+        x, y, z = xyz(q)
+        fd = oracle_mod.direct_forces(m, x, y, z, 1.0, 0.0)
+        tree = oracle_mod.Octree(m, method).init(x, y, z)
+        for th in thetas:
+            errs[th].append(_normalised_rms(oracle_mod, m, q, tree.forces(th * th, 1.0, 0.0), fd))
+    for th in thetas:
+        rec = recorded[f"dehnen{order}/{n}/{th:.1f}"]
+        med = float(np.median(errs[th]))
+        assert 0.6 * rec["p10"] <= med <= 1.6 * rec["p90"], (order, th, med, rec)
+
+
+@pytest.mark.parametrize("method,mult", [(20, 1), (21, 4), (22, 8)])
+def test_dehnen_on_insertion_and_morton_trees_agree(oracle_mod, method, mult):
+    """The insertion tree (octree_default) and the Morton tree share the root
+    cube, so Dehnen's method gives the same forces on both (to rounding): a
+    check of the generic-tree adapters, the Morton one being what the device
+    tree reproduces."""
+    m, q = plummer(3000, seed=11)
+    x, y, z = xyz(q)
+    fi = oracle_mod.Octree(m, method).init(x, y, z).forces(0.3, 1.0, 1e-4)
+    fm = oracle_mod.MortonTree(m, x, y, z, L=21).dehnen(1.0, 1e-4, 0.3, mult)
+    rel = np.linalg.norm(fi - fm, axis=1) / np.linalg.norm(fi, axis=1)
+    assert rel.max() < 1e-12
+
+
+def test_dehnen_converges_to_direct_sum(oracle_mod):
+    m, q = plummer(2000, seed=12)
+    x, y, z = xyz(q)
+    fd = oracle_mod.direct_forces(m, x, y, z, 1.0, 1e-4)
+    t = oracle_mod.MortonTree(m, x, y, z, L=21)
+    prev = None
+    for th in (0.8, 0.4, 0.2, 0.05):
+        f = t.dehnen(1.0, 1e-4, th * th, 4)
+        e = np.linalg.norm(f - fd) / np.linalg.norm(fd)
+        if prev is not None:
+            assert e < prev
+        prev = e
+    assert prev < 1e-5
