@@ -96,7 +96,37 @@ __global__ void roots_frontier_kernel(const SysScalars *__restrict__ ss, int nsy
   fout[slot] = make_int2(ss[s].root, ss[s].root);
 }
 
-// One generation of the dual traversal.
+__device__ __forceinline__ int64_t warp_incl_scan64(int64_t v, int lane) {
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const int64_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// Reserves `cnt` slots for this lane in a list shared by the grid: one atomic
+// per warp on the list's counter.  Returns the lane's first slot, or -1 when
+// the warp's slots would pass `cap` (the list overflowed).
+__device__ __forceinline__ int64_t warp_reserve(unsigned long long *counter, int64_t cnt,
+                                                int64_t cap, int lane, unsigned long long *flags,
+                                                unsigned long long flag) {
+  const int64_t incl = warp_incl_scan64(cnt, lane);
+  const int64_t total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+  int64_t base = 0;
+  if (lane == kWarp - 1 && total > 0) base = (int64_t)atomicAdd(counter, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, kWarp - 1);
+  if (total == 0) return 0;
+  if (base + total > cap) {
+    if (lane == kWarp - 1) atomicOr(flags, flag);
+    return -1;
+  }
+  return base + incl - cnt;
+}
+
+// One generation of the dual traversal.  Warps go through the input pairs 32
+// at a time; every lane classifies its pair, then the warp reserves the
+// output slots of all its lanes at once.
 __global__ void __launch_bounds__(256)
 dual_step_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *__restrict__ nin,
                  int64_t cap_in, int2 *__restrict__ fout, unsigned long long *nout, int64_t cap_out,
@@ -104,45 +134,64 @@ dual_step_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *
                  unsigned long long *flags) {
   // after an overflow the count exceeds what was written: read only the buffer
   const int64_t n_in = (int64_t)*nin < cap_in ? (int64_t)*nin : cap_in;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_in;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t a = fin[i].x, b = fin[i].y;
-    const double4 ca = ent_com(e, a), cb = ent_com(e, b);
-    if (ca.w == 0.0 || cb.w == 0.0) continue;
-    if (a == b) {
-      if (a >= e.n) continue;  // a body with itself
-      const int4 mt = e.meta[a];
-      const int k = node_nchild(mt);
-      const int64_t cnt = (int64_t)k * (k + 1) / 2;
-      const int64_t base = (int64_t)atomicAdd(nout, (unsigned long long)cnt);
-      if (base + cnt > cap_out) { atomicOr(flags, 1ull); continue; }
-      int64_t w = base;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); i0 < n_in;
+       i0 += stride) {
+    const int64_t i = i0 + lane;
+    // kind: 0 nothing, 1 children pairs of a self pair, 2 mutual, 3 open `o`
+    int kind = 0, k = 0;
+    int64_t a = 0, b = 0, o = 0, other = 0;
+    bool open_a = false;
+    int4 mt = make_int4(0, 0, 0, 0);
+    if (i < n_in) {
+      a = fin[i].x; b = fin[i].y;
+      const double4 ca = ent_com(e, a), cb = ent_com(e, b);
+      if (ca.w != 0.0 && cb.w != 0.0) {
+        if (a == b) {
+          if (a < e.n) {  // a body with itself is dropped
+            mt = e.meta[a];
+            k = node_nchild(mt);
+            kind = 1;
+          }
+        } else {
+          const double dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
+          const double dist2 = dx * dx + dy * dy + dz * dz;
+          const double ra = ent_rmax(e, a), rb = ent_rmax(e, b);
+          const double rs = ra + rb;
+          if (rs * rs <= theta2 * dist2) {
+            kind = 2;
+          } else {
+            open_a = ra >= rb;
+            o = open_a ? a : b;
+            other = open_a ? b : a;
+            if (o >= e.n) {
+              atomicOr(flags, 4ull);  // cannot happen: bodies have rmax 0
+            } else {
+              mt = e.meta[o];
+              k = node_nchild(mt);
+              kind = 3;
+            }
+          }
+        }
+      }
+    }
+    const int64_t n_out = kind == 1 ? (int64_t)k * (k + 1) / 2 : (kind == 3 ? k : 0);
+    const int64_t fo = warp_reserve(nout, n_out, cap_out, lane, flags, 1ull);
+    const int64_t mo = warp_reserve(nmut, kind == 2 ? 1 : 0, cap_mut, lane, flags, 2ull);
+    if (kind == 2 && mo >= 0) mut[mo] = make_int2((int)a, (int)b);
+    if (kind == 1 && fo >= 0) {
+      int64_t w = fo;
       for (int p = 0; p < k; ++p) {
         const int64_t cp = node_child(e, a, mt, p);
         for (int q = p; q < k; ++q) fout[w++] = make_int2((int)cp, (int)node_child(e, a, mt, q));
       }
-      continue;
     }
-    const double dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
-    const double dist2 = dx * dx + dy * dy + dz * dz;
-    const double ra = ent_rmax(e, a), rb = ent_rmax(e, b);
-    const double rs = ra + rb;
-    if (rs * rs <= theta2 * dist2) {
-      const int64_t m = (int64_t)atomicAdd(nmut, 1ull);
-      if (m < cap_mut) mut[m] = make_int2((int)a, (int)b);
-      else atomicOr(flags, 2ull);
-      continue;
-    }
-    const bool open_a = ra >= rb;
-    const int64_t o = open_a ? a : b, other = open_a ? b : a;
-    if (o >= e.n) { atomicOr(flags, 4ull); continue; }  // cannot happen: bodies have rmax 0
-    const int4 mt = e.meta[o];
-    const int k = node_nchild(mt);
-    const int64_t base = (int64_t)atomicAdd(nout, (unsigned long long)k);
-    if (base + k > cap_out) { atomicOr(flags, 1ull); continue; }
-    for (int q = 0; q < k; ++q) {
-      const int64_t c = node_child(e, o, mt, q);
-      fout[base + q] = open_a ? make_int2((int)c, (int)other) : make_int2((int)other, (int)c);
+    if (kind == 3 && fo >= 0) {
+      for (int q = 0; q < k; ++q) {
+        const int64_t c = node_child(e, o, mt, q);
+        fout[fo + q] = open_a ? make_int2((int)c, (int)other) : make_int2((int)other, (int)c);
+      }
     }
   }
 }
@@ -163,103 +212,122 @@ expand_kernel(const int2 *__restrict__ mut, int64_t np, int eb, uint64_t *__rest
   }
 }
 
-// Sum of the one-sided terms of every target, in source order.
+// One one-sided term (t <- s) added to f (3), h (6), tt (10).
+template <int ORDER>
+__device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 &ct, bool tnode,
+                                         int64_t s, double G, double eps2, double *f, double *h,
+                                         double *tt) {
+  const double4 cs = ent_com(e, s);
+  const double Ms = cs.w, Mt = ct.w;
+  const double dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
+  const double r2 = dx * dx + dy * dy + dz * dz + eps2;
+  if (r2 == 0.0) return;
+  const double rinv = 1.0 / sqrt(r2);
+  const double rinv2 = rinv * rinv;
+  const double rinv3 = rinv * rinv2;
+  const double D1x = -G * dx * rinv3, D1y = -G * dy * rinv3, D1z = -G * dz * rinv3;
+  if (ORDER < 4) {
+    f[0] = f[0] + Ms * D1x; f[1] = f[1] + Ms * D1y; f[2] = f[2] + Ms * D1z;
+    return;
+  }
+  const double rinv5 = rinv3 * rinv2, rinv7 = rinv5 * rinv2;
+  double D2[6], D3[10];
+  D2[0] = G * (3.0 * dx * dx * rinv5 - rinv3);
+  D2[1] = G * (3.0 * dy * dy * rinv5 - rinv3);
+  D2[2] = G * (3.0 * dz * dz * rinv5 - rinv3);
+  D2[3] = G * 3.0 * dx * dy * rinv5;
+  D2[4] = G * 3.0 * dx * dz * rinv5;
+  D2[5] = G * 3.0 * dy * dz * rinv5;
+  D3[0] = G * (-15.0 * dx * dx * dx * rinv7 + 9.0 * dx * rinv5);
+  D3[1] = G * (-15.0 * dx * dx * dy * rinv7 + 3.0 * dy * rinv5);
+  D3[2] = G * (-15.0 * dx * dx * dz * rinv7 + 3.0 * dz * rinv5);
+  D3[3] = G * (-15.0 * dx * dy * dy * rinv7 + 3.0 * dx * rinv5);
+  D3[4] = G * (-15.0 * dx * dy * dz * rinv7);
+  D3[5] = G * (-15.0 * dx * dz * dz * rinv7 + 3.0 * dx * rinv5);
+  D3[6] = G * (-15.0 * dy * dy * dy * rinv7 + 9.0 * dy * rinv5);
+  D3[7] = G * (-15.0 * dy * dy * dz * rinv7 + 3.0 * dz * rinv5);
+  D3[8] = G * (-15.0 * dy * dz * dz * rinv7 + 3.0 * dy * rinv5);
+  D3[9] = G * (-15.0 * dz * dz * dz * rinv7 + 9.0 * dz * rinv5);
+  double cq[3] = {0.0, 0.0, 0.0};
+  if (s < e.n) {  // a node's specific quadrupole; a body has none
+    const double *q = e.quad + 6 * s;
+    const double Q0 = q[0] / Ms, Q1 = q[1] / Ms, Q2 = q[2] / Ms, Q3 = q[3] / Ms, Q4 = q[4] / Ms,
+                 Q5 = q[5] / Ms;
+    cq[0] = Q0 * D3[0] + 2.0 * Q3 * D3[1] + 2.0 * Q4 * D3[2] + Q1 * D3[3] + 2.0 * Q5 * D3[4] +
+            Q2 * D3[5];
+    cq[1] = Q0 * D3[1] + 2.0 * Q3 * D3[3] + 2.0 * Q4 * D3[4] + Q1 * D3[6] + 2.0 * Q5 * D3[7] +
+            Q2 * D3[8];
+    cq[2] = Q0 * D3[2] + 2.0 * Q3 * D3[4] + 2.0 * Q4 * D3[5] + Q1 * D3[7] + 2.0 * Q5 * D3[8] +
+            Q2 * D3[9];
+  }
+  f[0] = f[0] + Ms * (D1x + 0.5 * cq[0]);
+  f[1] = f[1] + Ms * (D1y + 0.5 * cq[1]);
+  f[2] = f[2] + Ms * (D1z + 0.5 * cq[2]);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) h[q] = h[q] + Ms * D2[q];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) tt[q] = tt[q] + Ms * D3[q];
+  if (ORDER >= 8 && (tnode || s < e.n)) {
+    // octupole torque term (:1530-1557); a body's octupole is zero.
+    // C_jkl = Ms O_t - Mt O_s, components 0 xxx 1 xyy 2 xzz 3 yxx 4 yyy 5 yzz
+    // 6 zxx 7 zyy 8 zzz 9 xyz (the index map of :233-241)
+    const double *ot = tnode ? e.oct + 14 * t : nullptr;
+    const double *os = s < e.n ? e.oct + 14 * s : nullptr;
+    double C[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) C[q] = (ot ? Ms * ot[q] : 0.0) - (os ? Mt * os[q] : 0.0);
+    const double cx = C[0] + C[1] + C[2], cy = C[3] + C[4] + C[5], cz = C[6] + C[7] + C[8];
+    const double crx = C[0] * dx * dx + C[1] * dy * dy + C[2] * dz * dz +
+                       2.0 * (C[3] * dx * dy + C[6] * dx * dz + C[9] * dy * dz);
+    const double cry = C[3] * dx * dx + C[4] * dy * dy + C[5] * dz * dz +
+                       2.0 * (C[1] * dx * dy + C[9] * dx * dz + C[7] * dy * dz);
+    const double crz = C[6] * dx * dx + C[7] * dy * dy + C[8] * dz * dz +
+                       2.0 * (C[9] * dx * dy + C[2] * dx * dz + C[5] * dy * dz);
+    const double a3 = 3.0 * G * rinv5, a15 = 15.0 * G * rinv7;
+    f[0] = f[0] + 0.5 * (a3 * cx - a15 * crx) / Mt;
+    f[1] = f[1] + 0.5 * (a3 * cy - a15 * cry) / Mt;
+    f[2] = f[2] + 0.5 * (a3 * cz - a15 * crz) / Mt;
+  }
+}
+
+// Sum of the one-sided terms of every target, one warp per target: lane l
+// adds terms l, l + 32, ... of the target's source-ordered list, then the
+// lanes' sums are combined by a fixed butterfly, so the result depends only on
+// the target's own list.
 template <int ORDER>
 __global__ void __launch_bounds__(128)
 eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const uint64_t *__restrict__ keys,
             int eb, double G, double eps2, double *__restrict__ F, double *__restrict__ H,
             double *__restrict__ T) {
+  constexpr int NV = ORDER >= 4 ? 19 : 3;
   const uint64_t mask = (1ull << eb) - 1;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ne;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    double f[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0}, tt[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; t < ne; t += wstride) {
+    double v[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) v[q] = 0.0;
     const int kb = beg[t], ke = beg[t + 1];
     if (kb < ke) {
       const double4 ct = ent_com(e, t);
-      const double Mt = ct.w;
       const bool tnode = t < e.n;
-      for (int k = kb; k < ke; ++k) {
-        const int64_t s = (int64_t)(keys[k] & mask);
-        const double4 cs = ent_com(e, s);
-        const double Ms = cs.w;
-        const double dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
-        const double r2 = dx * dx + dy * dy + dz * dz + eps2;
-        if (r2 == 0.0) continue;
-        const double rinv = 1.0 / sqrt(r2);
-        const double rinv2 = rinv * rinv;
-        const double rinv3 = rinv * rinv2;
-        const double D1x = -G * dx * rinv3, D1y = -G * dy * rinv3, D1z = -G * dz * rinv3;
-        if (ORDER < 4) {
-          f[0] = f[0] + Ms * D1x; f[1] = f[1] + Ms * D1y; f[2] = f[2] + Ms * D1z;
-          continue;
-        }
-        const double rinv5 = rinv3 * rinv2, rinv7 = rinv5 * rinv2;
-        double D2[6], D3[10];
-        D2[0] = G * (3.0 * dx * dx * rinv5 - rinv3);
-        D2[1] = G * (3.0 * dy * dy * rinv5 - rinv3);
-        D2[2] = G * (3.0 * dz * dz * rinv5 - rinv3);
-        D2[3] = G * 3.0 * dx * dy * rinv5;
-        D2[4] = G * 3.0 * dx * dz * rinv5;
-        D2[5] = G * 3.0 * dy * dz * rinv5;
-        D3[0] = G * (-15.0 * dx * dx * dx * rinv7 + 9.0 * dx * rinv5);
-        D3[1] = G * (-15.0 * dx * dx * dy * rinv7 + 3.0 * dy * rinv5);
-        D3[2] = G * (-15.0 * dx * dx * dz * rinv7 + 3.0 * dz * rinv5);
-        D3[3] = G * (-15.0 * dx * dy * dy * rinv7 + 3.0 * dx * rinv5);
-        D3[4] = G * (-15.0 * dx * dy * dz * rinv7);
-        D3[5] = G * (-15.0 * dx * dz * dz * rinv7 + 3.0 * dx * rinv5);
-        D3[6] = G * (-15.0 * dy * dy * dy * rinv7 + 9.0 * dy * rinv5);
-        D3[7] = G * (-15.0 * dy * dy * dz * rinv7 + 3.0 * dz * rinv5);
-        D3[8] = G * (-15.0 * dy * dz * dz * rinv7 + 3.0 * dy * rinv5);
-        D3[9] = G * (-15.0 * dz * dz * dz * rinv7 + 9.0 * dz * rinv5);
-        double cq[3] = {0.0, 0.0, 0.0};
-        if (s < e.n) {  // a node's specific quadrupole; a body has none
-          const double *q = e.quad + 6 * s;
-          const double Q0 = q[0] / Ms, Q1 = q[1] / Ms, Q2 = q[2] / Ms, Q3 = q[3] / Ms,
-                       Q4 = q[4] / Ms, Q5 = q[5] / Ms;
-          cq[0] = Q0 * D3[0] + 2.0 * Q3 * D3[1] + 2.0 * Q4 * D3[2] + Q1 * D3[3] + 2.0 * Q5 * D3[4] +
-                  Q2 * D3[5];
-          cq[1] = Q0 * D3[1] + 2.0 * Q3 * D3[3] + 2.0 * Q4 * D3[4] + Q1 * D3[6] + 2.0 * Q5 * D3[7] +
-                  Q2 * D3[8];
-          cq[2] = Q0 * D3[2] + 2.0 * Q3 * D3[4] + 2.0 * Q4 * D3[5] + Q1 * D3[7] + 2.0 * Q5 * D3[8] +
-                  Q2 * D3[9];
-        }
-        f[0] = f[0] + Ms * (D1x + 0.5 * cq[0]);
-        f[1] = f[1] + Ms * (D1y + 0.5 * cq[1]);
-        f[2] = f[2] + Ms * (D1z + 0.5 * cq[2]);
+      for (int k = kb + lane; k < ke; k += kWarp)
+        add_term<ORDER>(e, t, ct, tnode, (int64_t)(keys[k] & mask), G, eps2, v, v + 3, v + 9);
 #pragma unroll
-        for (int q = 0; q < 6; ++q) h[q] = h[q] + Ms * D2[q];
+      for (int q = 0; q < NV; ++q) {
 #pragma unroll
-        for (int q = 0; q < 10; ++q) tt[q] = tt[q] + Ms * D3[q];
-        if (ORDER >= 8 && (tnode || s < e.n)) {
-          // octupole torque term (:1530-1557); a body's octupole is zero
-          // C_jkl = Ms O_t - Mt O_s over the index map of :233-241
-          const double *ot = tnode ? e.oct + 14 * t : nullptr;
-          const double *os = s < e.n ? e.oct + 14 * s : nullptr;
-          double C[10];
-#pragma unroll
-          for (int q = 0; q < 10; ++q) C[q] = (ot ? Ms * ot[q] : 0.0) - (os ? Mt * os[q] : 0.0);
-          // components: 0 xxx 1 xyy 2 xzz 3 yxx 4 yyy 5 yzz 6 zxx 7 zyy 8 zzz 9 xyz
-          const double cx = C[0] + C[1] + C[2], cy = C[3] + C[4] + C[5], cz = C[6] + C[7] + C[8];
-          const double crx = C[0] * dx * dx + C[1] * dy * dy + C[2] * dz * dz +
-                             2.0 * (C[3] * dx * dy + C[6] * dx * dz + C[9] * dy * dz);
-          const double cry = C[3] * dx * dx + C[4] * dy * dy + C[5] * dz * dz +
-                             2.0 * (C[1] * dx * dy + C[9] * dx * dz + C[7] * dy * dz);
-          const double crz = C[6] * dx * dx + C[7] * dy * dy + C[8] * dz * dz +
-                             2.0 * (C[9] * dx * dy + C[2] * dx * dz + C[5] * dy * dz);
-          const double a3 = 3.0 * G * rinv5, a15 = 15.0 * G * rinv7;
-          f[0] = f[0] + 0.5 * (a3 * cx - a15 * crx) / Mt;
-          f[1] = f[1] + 0.5 * (a3 * cy - a15 * cry) / Mt;
-          f[2] = f[2] + 0.5 * (a3 * cz - a15 * crz) / Mt;
-        }
+        for (int o = 16; o > 0; o >>= 1) v[q] = v[q] + __shfl_xor_sync(0xffffffffu, v[q], o);
       }
     }
+    if (lane == 0) {
 #pragma unroll
-    for (int q = 0; q < 3; ++q) F[3 * t + q] = f[q];
-    if (ORDER >= 4) {
+      for (int q = 0; q < 3; ++q) F[3 * t + q] = v[q];
+      if (ORDER >= 4) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q) H[6 * t + q] = h[q];
+        for (int q = 0; q < 6; ++q) H[6 * t + q] = v[3 + q];
 #pragma unroll
-      for (int q = 0; q < 10; ++q) T[10 * t + q] = tt[q];
+        for (int q = 0; q < 10; ++q) T[10 * t + q] = v[9 + q];
+      }
     }
   }
 }
@@ -429,7 +497,7 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
                      &b.sc->err, s);
   }
   exclusive_scan(d.cnt, d.beg, ne + 1, nullptr, nullptr, d.scan_tmp, s);
-  const int egrid = grid_for(ne, 128, 148 * 16);
+  const int egrid = grid_for(ne * kWarp, 128, 148 * 32);
   const double G = p.G, eps2 = p.eps2;
   if (p.order >= 8)
     eval_kernel<8><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.keys, eb, G, eps2, d.F, d.H, d.T);
