@@ -18,7 +18,9 @@ batching server against the plain single-system call:
   * batched -- 512 independent systems (N log-uniform in [1024, 65536], Plummer
     and uniform-density spheres): one batched build + walk (and its CUDA-graph
     replay) with autotuned group/leaf parameters against a loop of plain
-    calls.
+    calls;
+  * dehnen -- Dehnen's dual-tree method (FP64) on the accuracy system, with its
+    error on the same targets.
 
 The RMS relative error is measured against the FP64 direct sum on 16,384
 seeded targets; served results are checked equal (bit for bit) to the plain
@@ -152,18 +154,21 @@ class ClockSampler:
 
 def launches_per_evaluation(n, nsys=1, L=21):
     """Our kernel launches in one build + walk (the pipeline's launch sequence;
-    the ncu launch list shows 105 for one system of 2^20 bodies)."""
+    the ncu launch list shows 61 for one system of 2^20 bodies)."""
     scan = 3                                           # reduce, block scan, apply
-    sort_pass = 1 + scan + 1                           # upsweep, scan, downsweep
+
+    def sort(bits):                                    # digit histograms, their scan, passes
+        return 2 + math.ceil(bits / 8)
+
     keys = 3                                           # reduce, finalize, keys
-    particle_sort = math.ceil(3 * L / 8) * sort_pass
+    particle_sort = sort(3 * L)
     by_system = 0
     if nsys >= 2:
-        by_system = 1 + math.ceil(max(1, math.ceil(math.log2(nsys))) / 8) * sort_pass + 1
+        by_system = 1 + sort(max(1, math.ceil(math.log2(nsys)))) + 1
     first_bits = 1
     while (1 << first_bits) <= n:
         first_bits += 1
-    node_sort = math.ceil((first_bits + 5) / 8) * sort_pass
+    node_sort = sort(first_bits + 5)
     # karras, mark, scan, count, compact keys, node sort, bin2cn, records, levels, roots
     tree = 2 + scan + 1 + 1 + node_sort + 1 + 1 + 1 + 1
     upward = 22
@@ -342,6 +347,31 @@ def run_ours(args):
                             "reference_walk_rms_rel": err_ref["rms_rel"],
                             "meets_1e-3": err["rms_rel"] <= 1e-3,
                             "served": "identical to plain (bitwise)" if same else "DIFFERS"}
+
+        # ---- Dehnen's dual-tree method on the same system (methods 20/21/22) ----
+        pd = _lib.default_params(theta=THETA, eps=EPS, order=args.order,
+                                 precision=_lib.BH_PREC_DEHNEN)
+        dsys = BHSystem(local)
+        dout = torch.empty(3 * n, dtype=torch.float64, device=dev)
+        dsys.forces(mK, xK, yK, zK, pd, out=dout)  # sizes its pair lists
+        td = []
+        for _ in range(3):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            dsys.forces(mK, xK, yK, zK, pd, out=dout)
+            b.record(stream)
+            b.synchronize()
+            td.append(a.elapsed_time(b))
+        derr = error_stats(dout.view(3, n).T[ttg].cpu().numpy(), fd, mh[tg], qh[tg])
+        line["dehnen"] = {"value": n / (statistics.mean(td) * 1e-3), "unit": "forces/s",
+                          "ms_per_call": statistics.mean(td), "theta": THETA, "order": args.order,
+                          "rms_rel": derr["rms_rel"], "max_rel": derr["max_rel"],
+                          "note": "FP64 build + dual traversal + terms + downward pass, same "
+                                  "system and targets as the accuracy check"}
+        dsys.close()
+        del dout
 
         # ---- roofline of the walk (dominant kernel) ----
         p.count_stats = 1

@@ -12,7 +12,7 @@
 // Limits and behaviour:
 //  * at most BH_NOALLOC_MAX_N bodies (8192); larger n is rejected with
 //    BH_ERR_INVALID and a message;
-//  * the array (about 5.7 MB) lives on every device on which this library's
+//  * the array (about 5.8 MB) lives on every device on which this library's
 //    module holding it is loaded, until the process exits;
 //  * the first call on a device looks the array's device address up
 //    (cudaGetSymbolAddress, with that device current) and keeps it; later
@@ -36,7 +36,7 @@
 namespace {
 
 constexpr int64_t kMaxN = BH_NOALLOC_MAX_N;
-constexpr int64_t kSlots = 512;       // warp slots of the walk (128 blocks of 4 warps)
+constexpr int64_t kSlots = 512;       // stacks of the walk (512 persistent one-warp blocks)
 constexpr int64_t kStackCap = 1024;   // stack entries per warp slot
 constexpr int64_t kItems = (kMaxN + bh::kRedChunk - 1) / bh::kRedChunk;  // reduction items
 constexpr int kNumBufs = 36;

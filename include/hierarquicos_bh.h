@@ -201,7 +201,7 @@ int bh_system_reference_targets(bh_system *sys, const bh_params *p, const int64_
  * memory (their memory belongs to another allocator, a cudaMalloc would stall
  * their time-step loop, or their host forbids it).  No counterpart in the
  * reference.  Device inputs and output as bh_system_forces; everything else
- * comes from one fixed device array of about 5.7 MB inside the library, so n
+ * comes from one fixed device array of about 5.8 MB inside the library, so n
  * is limited to BH_NOALLOC_MAX_N (larger n: BH_ERR_INVALID).  The first call on
  * a device looks that array up; all calls on a device share it, so calls that
  * overlap on the GPU race: run them one after another.  Synchronous. */
