@@ -68,7 +68,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--bodies", type=int, default=N_DEFAULT, dest="n")
     ap.add_argument("--order", type=int, default=ORDER)
-    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--precision", type=int, default=0,
+                    help="0 FP32 group walk, 1 FP64 group walk, 2 per-target FP64, 3 Dehnen")
     ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--leaf-cap", type=int, default=8)
     ap.add_argument("--group-span", type=int, default=0)
@@ -254,7 +255,7 @@ def run_ours(args):
                        "n_per_request": n, "requests_per_gpu": K, "theta": THETA, "eps": EPS,
                        "order": args.order,
                        "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk",
-                                2: "fp64 per-target"}[args.precision],
+                                2: "fp64 per-target", 3: "fp64 dehnen dual tree"}[args.precision],
                        "group_size": args.group_size, "leaf_cap": args.leaf_cap,
                        "group_span": args.group_span or 2 * args.group_size, "mac": p.mac,
                        "keys": "63-bit, strict",
