@@ -77,6 +77,9 @@ def parse():
                     help="group walk acceptance: 0 box distance, 1 box or every member's own MAC")
     ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--batch-systems", type=int, default=512)
+    ap.add_argument("--split-system", action="store_true",
+                    help="strong scaling: every rank takes the same system and walks its share of "
+                         "the target groups; one all-reduce combines them (implies --no-extras)")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain timed calls only (no serving, error check, e2e, batch or CPU baseline)")
     return ap.parse_args()
@@ -214,9 +217,14 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    # K timed + W warm-up systems, drawn on the device
-    systems = [device_workload(n, seed=1000 + 97 * rank + i) for i in range(K + W)]
+    # K timed + W warm-up systems, drawn on the device (the same systems on
+    # every rank when one system is split over the ranks)
+    rank_seed = 0 if args.split_system else 97 * rank
+    systems = [device_workload(n, seed=1000 + rank_seed + i) for i in range(K + W)]
     out = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    if args.split_system:
+        args.no_extras = True
+        return run_split(args, p, systems, out, flush, dev, local, rank, world)
 
     # ---- plain: one call per system ----
     sysm = BHSystem(local)
@@ -462,6 +470,55 @@ def run_ours(args):
         if rank == 0 and world == 1:
             m0, q0 = workload(n, seed=1000)
             line["cpu_baseline"] = cpu_baseline(n, m0, q0, args.order, samples=32768)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_split(args, p, systems, out, flush, dev, local, rank, world):
+    """One system per step split over the ranks: each rank builds it whole,
+    walks its range of target groups and the ranks' outputs are summed (one
+    NCCL all-reduce inside the timed step); strong scaling."""
+    import torch
+    import torch.distributed as dist
+
+    from hierarquicos_b200.shard import sharded_forces
+    from hierarquicos_b200.system import BHSystem
+
+    n, K, W = args.n, args.steps, args.warmup
+    stream = torch.cuda.current_stream()
+    sysm = BHSystem(local)
+    for i in range(W):
+        sharded_forces(sysm, *systems[K + i], p, out=out, rank=rank, world=world)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    times = []
+    with ClockSampler(local) as clocks:
+        for i in range(K):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            sharded_forces(sysm, *systems[i], p, out=out, rank=rank, world=world)
+            b.record(stream)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+    ms = dist_max(float(sum(times)), dev, world) / K
+    line = {"metric": METRIC, "value": n / (ms * 1e-3), "unit": "forces/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 walk (Kahan), f64 keys/moments",
+            "data": "synthetic (seeded Hernquist ICs drawn on the device)",
+            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, one system "
+                                   f"split over {world} ranks", "theta": THETA, "eps": EPS,
+                       "order": args.order, "parallelism": f"target groups split x{world}, "
+                                                           "all-reduce of the forces",
+                       "l2": "flushed (256 MiB write) before every step"},
+            "clocks": clocks.summary(),
+            "gpu_launches": launches_per_evaluation(n) * K}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -33,6 +33,7 @@ EXPORTED = [
     "bh_params_default", "bh_version", "bh_last_error", "bh_compute_forces",
     "bh_compute_forces_ex", "bh_compute_forces_direct", "bh_direct_targets_device",
     "bh_system_create", "bh_system_destroy", "bh_system_build", "bh_system_walk",
+    "bh_system_walk_groups",
     "bh_system_forces", "bh_system_sync", "bh_system_info", "bh_system_get_keys",
     "bh_system_get_nodes", "bh_system_get_groups", "bh_system_get_stats",
     "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
@@ -96,6 +97,7 @@ def lib():
             "bh_system_destroy": [_vp],
             "bh_system_build": [_vp, _vp, _vp, _vp, _vp, _i64, C.POINTER(BHParams), _vp],
             "bh_system_walk": [_vp, C.POINTER(BHParams), _vp, _vp],
+            "bh_system_walk_groups": [_vp, C.POINTER(BHParams), _i64, _i64, _vp, _vp],
             "bh_system_forces": [_vp, _vp, _vp, _vp, _vp, _i64, C.POINTER(BHParams), _vp, _vp],
             "bh_system_sync": [_vp, _vp],
             "bh_system_info": [_vp, C.POINTER(_i64), C.POINTER(_i), C.POINTER(_i64),

@@ -31,6 +31,7 @@ struct bh_system {
   int walked = 0;
   bh_params walk_p{};
   double *walk_out = nullptr;
+  int walk_g0 = 0, walk_g1 = -1;  // its target groups (bh_system_walk_groups)
   // captured build + walk of the current layout
   cudaGraphExec_t graph = nullptr;
   // pinned staging of the layout's reduction items; the event marks the end
@@ -329,7 +330,9 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
 
 // the walk of the whole batch, enqueued without host synchronisation
 int enqueue_walk(bh_system *s, const bh_params *p, double *d_out, cudaStream_t st) {
-  const bh::WalkParams w = walk_params(p, s->order);
+  bh::WalkParams w = walk_params(p, s->order);
+  w.g_begin = s->walk_g0;
+  w.g_end = s->walk_g1;
   if (w.count_stats) cudaMemsetAsync(s->b.stats, 0, 4 * sizeof(unsigned long long), st);
   if (p->precision == BH_PREC_DEHNEN) {
     switch (bh::run_dehnen(s->n, w, s->b, s->dehnen, d_out, st)) {
@@ -562,7 +565,10 @@ int bh_system_build_batch(bh_system *s, const double *d_m, const double *d_x,
   return build_common(s, d_m, d_x, d_y, d_z, offsets, nsys, p, (cudaStream_t)stream);
 }
 
-int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream) {
+// The walk over target groups [g0, g1) (g1 < 0: all), remembered so that a
+// repeated walk (strict-key rebuild, stack growth) covers the same groups.
+static int walk_impl(bh_system *s, const bh_params *p, int g0, int g1, double *d_out,
+                     void *stream) {
   if (!s) return set_err(BH_ERR_INVALID, "sys is NULL");
   if (!s->built) return set_err(BH_ERR_NOT_BUILT, "walk before build");
   int rc = check_params(p, s->n);
@@ -570,6 +576,8 @@ int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream
   if (p->order > s->order) return set_err(BH_ERR_INVALID, "order %d above the built order %d", p->order, s->order);
   if (!d_out) return set_err(BH_ERR_INVALID, "NULL output");
   BH_CUDA(cudaSetDevice(s->device));
+  s->walk_g0 = g0;
+  s->walk_g1 = g1;
   rc = enqueue_walk(s, p, d_out, (cudaStream_t)stream);
   if (rc) return rc;
   BH_CUDA(cudaGetLastError());
@@ -577,6 +585,21 @@ int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream
   s->walk_p = *p;
   s->walk_out = d_out;
   return BH_OK;
+}
+
+int bh_system_walk(bh_system *s, const bh_params *p, double *d_out, void *stream) {
+  return walk_impl(s, p, 0, -1, d_out, stream);
+}
+
+int bh_system_walk_groups(bh_system *s, const bh_params *p, int64_t g_begin, int64_t g_end,
+                          double *d_out, void *stream) {
+  if (!p) return set_err(BH_ERR_INVALID, "params is NULL");
+  if (p->precision != BH_PREC_FP32 && p->precision != BH_PREC_FP64)
+    return set_err(BH_ERR_INVALID, "a range of target groups needs the group walk (FP32 or FP64)");
+  if (g_begin < 0 || g_end < g_begin || g_end > ((int64_t)1 << 30))
+    return set_err(BH_ERR_INVALID, "group range [%lld, %lld) invalid", (long long)g_begin,
+                   (long long)g_end);
+  return walk_impl(s, p, (int)g_begin, (int)g_end, d_out, stream);
 }
 
 int bh_system_sync(bh_system *s, void *stream) {

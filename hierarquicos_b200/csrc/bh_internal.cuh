@@ -177,6 +177,7 @@ struct WalkParams {
   int leaf_cap;
   int count_stats;
   int mac;         // 0 box distance, 1 box distance or every member's own MAC
+  int g_begin = 0, g_end = -1;  // target groups walked: [g_begin, g_end), g_end < 0 = all
 };
 // Work buffers of Dehnen's dual-tree method (allocated on first use, grown on
 // demand): entity arrays for nodes and bodies (2n entities), the pair

@@ -94,6 +94,7 @@ struct WalkArgs {
   int64_t n;
   double theta2, G, eps2;
   int out_kind, leaf_cap, count_stats, mac;
+  int g_begin, g_end;  // groups walked: [g_begin, g_end), g_end < 0 = all
 };
 
 template <typename T>
@@ -722,12 +723,12 @@ group_walk_kernel(WalkArgs a) {
   const int lane = threadIdx.x;
   int32_t *stack = a.stack + (int64_t)blockIdx.x * a.stack_cap;
   const int stack_cap = (int)a.stack_cap;
-  const int ngroups = a.sc->n_groups;
+  const int ngroups = a.g_end >= 0 ? min(a.g_end, a.sc->n_groups) : a.sc->n_groups;
   const T theta2 = (T)a.theta2;
   WalkCounters wc;
   for (;;) {
     int g = 0;
-    if (lane == 0) g = atomicAdd(a.cursor, 1);
+    if (lane == 0) g = a.g_begin + atomicAdd(a.cursor, 1);
     g = __shfl_sync(kFull, g, 0);
     if (g >= ngroups) break;
     const int gf = a.g_first[g];
@@ -945,6 +946,7 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   a.theta2 = p.theta2; a.G = p.G; a.eps2 = p.eps2;
   a.out_kind = p.out_kind; a.leaf_cap = p.leaf_cap; a.count_stats = p.count_stats;
   a.mac = p.mac;
+  a.g_begin = p.g_begin; a.g_end = p.g_end;
   return a;
 }
 

@@ -72,11 +72,18 @@ class BHSystem:
                                     C.byref(p), _stream()))
         return self
 
-    def walk(self, params: BHParams | None = None, out: torch.Tensor | None = None, **kw):
+    def walk(self, params: BHParams | None = None, out: torch.Tensor | None = None,
+             groups: tuple[int, int] | None = None, **kw):
+        """Group walk into ``out``; ``groups=(g0, g1)`` walks only target groups
+        [g0, g1) and leaves the other bodies' entries of ``out`` as they are."""
         p = params if params is not None else default_params(**kw)
         if out is None:
             out = torch.empty(3 * self.n, dtype=torch.float64, device=f"cuda:{self.device}")
-        check(lib().bh_system_walk(self._h, C.byref(p), _dptr(out), _stream()))
+        if groups is None:
+            check(lib().bh_system_walk(self._h, C.byref(p), _dptr(out), _stream()))
+        else:
+            check(lib().bh_system_walk_groups(self._h, C.byref(p), int(groups[0]), int(groups[1]),
+                                              _dptr(out), _stream()))
         return out
 
     def sync(self):

@@ -122,6 +122,16 @@ int bh_system_build(bh_system *sys, const double *d_m, const double *d_x, const 
  * ORIGINAL particle order.  Asynchronous. */
 int bh_system_walk(bh_system *sys, const bh_params *p, double *d_out, void *stream);
 
+/* The group walk over target groups [g_begin, g_end) only (groups are Morton-
+ * contiguous runs of bodies; bh_system_info gives their number; g_end beyond
+ * it is clamped): forces of those groups' bodies are written, all others are
+ * left as they are.  For sharding one system's targets over GPUs: every rank
+ * builds the whole tree, walks its range of groups into a zeroed d_out, and a
+ * sum over the ranks (one all-reduce) gives the full result, bit for bit the
+ * single-GPU walk's.  FP32 / FP64 group walk only.  Asynchronous. */
+int bh_system_walk_groups(bh_system *sys, const bh_params *p, int64_t g_begin, int64_t g_end,
+                          double *d_out, void *stream);
+
 /* build + walk + bh_system_sync: the device-array form of bh_compute_forces. */
 int bh_system_forces(bh_system *sys, const double *d_m, const double *d_x, const double *d_y,
                      const double *d_z, int64_t n, const bh_params *p, double *d_out,

@@ -145,3 +145,28 @@ def test_results_independent_of_call_history(api):
     api.compute_forces(m2, *xyz(q2), 0.7, 1.0, 0.0, order=8)
     f2 = api.compute_forces(m, x, y, z, 0.5, 1.0, 0.01, True)
     assert np.array_equal(f1, f2)
+
+
+@pytest.mark.parametrize("parts", [2, 3, 8])
+def test_walk_over_group_ranges_equals_full_walk(parts):
+    """Sharding one system's targets: walking the target groups in disjoint
+    ranges, each into a zeroed output, and summing the outputs gives the full
+    walk bit for bit (the combine step of a multi-GPU run)."""
+    import torch
+
+    from hierarquicos_b200.shard import group_range
+    from hierarquicos_b200.system import BHSystem
+
+    m, q = plummer(20000, seed=21)
+    x, y, z = xyz(q)
+    s = BHSystem()
+    kw = dict(theta=0.5, eps=0.01, order=4)
+    full = s.forces(m, x, y, z, **kw).clone()
+    ng = s.info()["n_groups"]
+    total = torch.zeros_like(full)
+    for r in range(parts):
+        out = torch.zeros_like(full)
+        s.walk(out=out, groups=group_range(ng, r, parts), **kw)
+        s.sync()
+        total += out
+    assert torch.equal(total, full)

@@ -71,3 +71,66 @@ def test_reference_arm_other_ranks_exit_without_work(rank):
     r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--bodies", "4096"], cwd=ROOT,
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_group_ranges_partition_the_groups():
+    sys.path.insert(0, ROOT)
+    from hierarquicos_b200.shard import group_range
+
+    for n_groups in (0, 1, 5, 16384, 16385):
+        for world in (1, 2, 3, 8):
+            seen = []
+            for r in range(world):
+                g0, g1 = group_range(n_groups, r, world)
+                assert 0 <= g0 <= g1 <= n_groups
+                assert g1 - g0 in (n_groups // world, n_groups // world + 1)
+                seen.extend(range(g0, g1))
+            assert seen == list(range(n_groups))
+
+
+def _shard_worker(rank, world, port, q):
+    """Each rank fills only its groups' bodies (zeros elsewhere); the sum over
+    the ranks must be every body's value exactly."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, ROOT)
+    from hierarquicos_b200.shard import combine, group_range
+
+    rng = np.random.default_rng(7)
+    n, n_groups = 1000, 37
+    g_first = np.sort(rng.choice(np.arange(1, n), n_groups - 1, replace=False))
+    g_first = np.concatenate([[0], g_first, [n]])
+    full = rng.standard_normal(3 * n)  # the same "forces" on every rank
+    perm = rng.permutation(n)          # sorted position -> original index
+    g0, g1 = group_range(n_groups, rank, world)
+    out = torch.zeros(3 * n, dtype=torch.float64)
+    for i in range(g_first[g0], g_first[g1]):
+        o = perm[i]
+        for k in range(3):
+            out[k * n + o] = full[k * n + o]
+    combine(out)
+    ok = bool(np.array_equal(out.numpy(), full))
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, ok))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_outputs_combine_to_the_full_result(world):
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(res.values()), res
