@@ -202,6 +202,15 @@ __device__ __forceinline__ float fast_rsqrt(float x) {
 }
 __device__ __forceinline__ double fast_rsqrt(double x) { return rsqrt(x); }
 
+// (2^-level)^2 = 2^(-2 level), exact, from the exponent bits (level <= 21)
+template <typename T> __device__ __forceinline__ T pow2_neg2(int level);
+template <> __device__ __forceinline__ float pow2_neg2<float>(int level) {
+  return __int_as_float((127 - 2 * level) << 23);
+}
+template <> __device__ __forceinline__ double pow2_neg2<double>(int level) {
+  return __longlong_as_double((long long)(1023 - 2 * level) << 52);
+}
+
 // Smallest r^2 of a body pair when there is no softening: a body meets itself
 // (d = 0, contribution exactly 0) and exactly coincident bodies contribute 0;
 // r^-3 stays finite in T.
@@ -525,6 +534,7 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
 #pragma unroll
       for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = make_float2(0.0f, 0.0f);
       const int np = (nc + 1) >> 1;
+#pragma unroll 2
       for (int j = 0; j < np; ++j) {
         const float4 *st = reinterpret_cast<const float4 *>(S.stage) + j * (W / 2);
         float2 cw[W];
@@ -592,7 +602,7 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
       const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
       const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
       const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
-      size2 = (T)ldexp(1.0, -2 * mt.z);
+      size2 = pow2_neg2<T>(mt.z);
       if (size2 <= theta2 * d2) {
         cls = 1;
       } else {
@@ -665,7 +675,9 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
     int rf = 0, rn = 0;
     if (cls == 2) { rf = mt.x; rn = mt.y; }
     bool first_pass = true;
-    for (;;) {
+    // nothing to queue on any lane (the common case): no scan
+    for (bool any = __ballot_sync(kFull, rn > 0 || (cls == 3 && npc > 0)) != 0u; any;
+         any = __ballot_sync(kFull, rn > 0) != 0u) {
       int give;
       if (first_pass && cls == 3) give = npc;
       else give = min(rn, kBodyPerLane);
