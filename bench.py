@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--group-span", type=int, default=0)
     ap.add_argument("--mac", type=int, default=None,
                     help="group walk acceptance: 0 box distance, 1 box or every member's own MAC")
+    ap.add_argument("--pipeline", type=int, default=None,
+                    help="FP32 walk: 0 one warp per group, 1 producer/consumer warp teams")
     ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--split-system", action="store_true",
@@ -214,6 +216,8 @@ def run_ours(args):
                             group_span=args.group_span)
     if args.mac is not None:
         p.mac = args.mac
+    if args.pipeline is not None:
+        p.pipeline = args.pipeline
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -265,7 +269,7 @@ def run_ours(args):
                        "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk",
                                 2: "fp64 per-target", 3: "fp64 dehnen dual tree"}[args.precision],
                        "group_size": args.group_size, "leaf_cap": args.leaf_cap,
-                       "group_span": args.group_span or 2 * args.group_size, "mac": p.mac,
+                       "group_span": args.group_span or 2 * args.group_size, "mac": p.mac, "pipeline": p.pipeline,
                        "keys": "63-bit, strict",
                        "l2": "plain: flushed (256 MiB write) before every call; served: every request "
                              "touches > 500 MB of distinct data (inputs larger than L2)",

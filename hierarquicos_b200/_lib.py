@@ -53,7 +53,7 @@ class BHParams(C.Structure):
         ("order", C.c_int), ("out_kind", C.c_int), ("depth", C.c_int), ("precision", C.c_int),
         ("amp", C.c_double), ("group_size", C.c_int), ("leaf_cap", C.c_int),
         ("com_mode", C.c_int), ("strict_keys", C.c_int), ("count_stats", C.c_int),
-        ("group_span", C.c_int), ("mac", C.c_int), ("reserved", C.c_int * 1),
+        ("group_span", C.c_int), ("mac", C.c_int), ("pipeline", C.c_int),
     ]
 
 

@@ -109,8 +109,7 @@ def tune(m, x, y, z, offsets, params: BHParams | None = None, reps: int = 2,
         if hit:
             p = default_params()
             for f, _ in BHParams._fields_:
-                if f != "reserved":
-                    setattr(p, f, getattr(p0, f))
+                setattr(p, f, getattr(p0, f))
             p.group_size, p.group_span, p.leaf_cap = hit["group_size"], hit["group_span"], hit["leaf_cap"]
             _memory[key] = hit
             return p, dict(hit, cached=True)
@@ -135,8 +134,7 @@ def tune(m, x, y, z, offsets, params: BHParams | None = None, reps: int = 2,
     for g, span, lc in cands:
         p = default_params()
         for f, _ in BHParams._fields_:
-            if f != "reserved":
-                setattr(p, f, getattr(p0, f))
+            setattr(p, f, getattr(p0, f))
         p.group_size, p.group_span, p.leaf_cap = g, span, lc
         sysm.forces_batch(m, x, y, z, off, p, out=out)  # warm-up (and growth)
         ms = _time_config(sysm, m, x, y, z, off, p, out, reps)
@@ -155,7 +153,6 @@ def tune(m, x, y, z, offsets, params: BHParams | None = None, reps: int = 2,
         _store(key, {k: rep[k] for k in ("group_size", "group_span", "leaf_cap", "ms", "rms", "key")})
     p = default_params()
     for f, _ in BHParams._fields_:
-        if f != "reserved":
-            setattr(p, f, getattr(p0, f))
+        setattr(p, f, getattr(p0, f))
     p.group_size, p.group_span, p.leaf_cap = best["group_size"], best["group_span"], best["leaf_cap"]
     return p, rep

@@ -269,6 +269,7 @@ int check_params(const bh_params *p, int64_t n) {
   if (p->group_span != 0 && (p->group_span < p->group_size || p->group_span > (1 << 20)))
     return set_err(BH_ERR_INVALID, "group_span must be 0 or in [group_size, 2^20]");
   if (p->mac != 0 && p->mac != 1) return set_err(BH_ERR_INVALID, "mac must be 0 or 1");
+  if (p->pipeline != 0 && p->pipeline != 1) return set_err(BH_ERR_INVALID, "pipeline must be 0 or 1");
   return BH_OK;
 }
 
@@ -279,6 +280,8 @@ int status_from_device(bh_system *s) {
     return set_err(BH_ERR_NONFINITE, "non-finite position or mass, or total mass <= 0");
   if (e & bh::kErrDuplicates)
     return set_err(BH_ERR_DUPLICATES, "depth 0: coincident bodies never get distinct keys");
+  if (e & bh::kErrTimeout)
+    return set_err(BH_ERR_INTERNAL, "a bounded wait inside a kernel gave up (flags 0x%x)", e);
   if (e & (bh::kErrIndex | bh::kErrChildren))
     return set_err(BH_ERR_INTERNAL, "internal tree check failed (flags 0x%x)", e);
   if (e & bh::kErrStackOverflow)
@@ -325,6 +328,7 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
   w.leaf_cap = p->leaf_cap;
   w.count_stats = p->count_stats;
   w.mac = p->mac;
+  w.pipeline = p->pipeline;
   return w;
 }
 

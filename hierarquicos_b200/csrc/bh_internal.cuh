@@ -23,6 +23,7 @@ enum DeviceError : int {
   kErrIndex = 1 << 2,          // internal index out of range (a bug)
   kErrDuplicates = 1 << 3,     // automatic depth impossible: coincident bodies
   kErrChildren = 1 << 4,       // more than 8 children (a bug)
+  kErrTimeout = 1 << 5,        // a bounded wait inside a kernel gave up
 };
 
 // A batch is a set of independent systems stored back to back: system s owns
@@ -145,7 +146,7 @@ inline int grid_for(int64_t n, int threads, int cap) {
 // stable LSD radix sort of (key, value) pairs over bits [0, bits); the
 // result ends in (k0, v0).  n_dev, when given, holds the element count on the
 // device (n is then an upper bound).  A look-back wait that gives up sets
-// kErrIndex in *err (device).
+// kErrTimeout in *err (device).
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
                       const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s);
 // scratch of the radix sort, in int32 entries: digit counts of 8 passes x 256
@@ -177,6 +178,7 @@ struct WalkParams {
   int leaf_cap;
   int count_stats;
   int mac;         // 0 box distance, 1 box distance or every member's own MAC
+  int pipeline = 0;  // FP32 walk: 0 one warp per group, 1 producer/consumer warps
   int g_begin = 0, g_end = -1;  // target groups walked: [g_begin, g_end), g_end < 0 = all
 };
 // Work buffers of Dehnen's dual-tree method (allocated on first use, grown on

@@ -198,7 +198,7 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
     while (j >= 0) {
       const uint64_t w = ld_relaxed(tiles + (int64_t)j * kRadix + d);
       if ((w & ~kTileValue) == 0) {
-        if (++spins > kLookbackSpins) { atomicOr(err, kErrIndex); break; }
+        if (++spins > kLookbackSpins) { atomicOr(err, kErrTimeout); break; }
         continue;
       }
       excl += (int64_t)(w & kTileValue);

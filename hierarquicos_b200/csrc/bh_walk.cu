@@ -95,6 +95,7 @@ struct WalkArgs {
   double theta2, G, eps2;
   int out_kind, leaf_cap, count_stats, mac;
   int g_begin, g_end;  // groups walked: [g_begin, g_end), g_end < 0 = all
+  int pipeline;        // FP32: producer/consumer warp teams
 };
 
 template <typename T>
@@ -374,6 +375,154 @@ struct WalkCounters {
   int err = 0;
 };
 
+// The tree walk of one group (the box-distance MAC of octree_default.f90
+// :1927-1936, optionally with every member's own MAC): accepted nodes are
+// queued as cells and the bodies of opened leaves and lone particles as
+// bodies; eval_cells(end, k) / eval_bodies(end, k) consume the k queue entries
+// that end at position `end`, 32 at a time and the remainders at the end.
+// Positions are relative to the group centre gc in units of the root side.
+template <typename T, int TPL, typename CellsFn, typename BodiesFn>
+__device__ __forceinline__ void tree_walk(const WalkArgs &a, int *cellq, int *bodyq,
+                                          int32_t *stack, int stack_cap, int gf, int gn, int root,
+                                          const double gc[3], double inv_s, const T blo[3],
+                                          const T bhi[3], T theta2, T inv_theta2, T diag, T rad,
+                                          const T (&rx)[TPL], const T (&ry)[TPL],
+                                          const T (&rz)[TPL], WalkCounters &wc,
+                                          CellsFn &&eval_cells, BodiesFn &&eval_bodies) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned lt = (1u << lane) - 1u;
+  int top = 1, ncell = 0, nbody = 0;
+  // a tree visits every node at most once per group: more tests than nodes
+  // means a malformed tree, and the walk stops with an error instead of
+  // looping
+  const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
+  int64_t group_tests = 0;
+  if (root < 0) top = 0;  // a lone body: no tree, no force
+  if (lane == 0) stack[0] = root;
+  __syncwarp();
+  while (top > 0) {
+    if (group_tests > max_tests) { wc.err |= kErrIndex; break; }
+    const int take = min(top, kWarp);
+    const int base = top - take;
+    const int node = lane < take ? stack[base + lane] : -1;
+    top = base;
+    __syncwarp();
+    int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
+    int4 mt = make_int4(0, 0, 0, 0);
+    T dx = (T)0, dy = (T)0, dz = (T)0, size2 = (T)0;
+    bool cand = false;
+    if (node >= 0) {
+      mt = a.meta[node];
+      const double4 c = a.com[node];
+      dx = (T)((c.x - gc[0]) * inv_s); dy = (T)((c.y - gc[1]) * inv_s); dz = (T)((c.z - gc[2]) * inv_s);
+      const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
+      const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
+      const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
+      const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
+      size2 = pow2_neg2<T>(mt.z);
+      if (size2 <= theta2 * d2) {
+        cls = 1;
+      } else {
+        cls = (mt.y <= a.leaf_cap || mt.w == 0) ? 2 : 3;
+        if (a.mac == 1 && (mt.x + mt.y <= gf || mt.x >= gf + gn)) {
+          // holds no member: accept when every member passes its own MAC.
+          // Every member is at least |c| - rad from the centre of mass (the
+          // sphere bound); otherwise the members are tested one by one below
+          // if the nearest of them (at most `diag` beyond the box) may pass.
+          const T reach = sqrt(size2 * inv_theta2);
+          const T dc = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
+          if (dc - rad >= reach) {
+            cls = 1;
+          } else {
+            const T r2 = reach - diag;
+            cand = r2 <= (T)0 || r2 * r2 <= d2;
+          }
+        }
+      }
+    }
+    // members' own MAC (morton_octree.f90:701-706: size^2 <= theta^2 d^2 with
+    // d from the member to the centre of mass), all members at once
+    for (unsigned pend = __ballot_sync(kFull, cand); pend; pend &= pend - 1) {
+      const int src = __ffs(pend) - 1;
+      const T cx = __shfl_sync(kFull, dx, src), cy = __shfl_sync(kFull, dy, src),
+              cz = __shfl_sync(kFull, dz, src), cs2 = __shfl_sync(kFull, size2, src);
+      T dmin = (T)INFINITY;
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        const T ux = cx - rx[t], uy = cy - ry[t], uz = cz - rz[t];
+        dmin = min(dmin, fma(ux, ux, fma(uy, uy, uz * uz)));
+      }
+      dmin = warp_min(dmin);
+      if (lane == src && cs2 <= theta2 * dmin) cls = 1;
+    }
+    wc.tests += take;
+    group_tests += take;
+    // cells
+    const unsigned cm = __ballot_sync(kFull, cls == 1);
+    if (cls == 1) cellq[ncell + __popc(cm & lt)] = node;
+    ncell += __popc(cm);
+    // children of opened internal nodes
+    int32_t ch[8];
+    int nnc = 0, npc = 0;
+    if (cls == 3) {
+      const int4 *cp = reinterpret_cast<const int4 *>(a.child + 8 * (int64_t)node);
+      const int4 c0 = cp[0], c1 = cp[1];
+      ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
+      ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c < mt.w) { if (ch[c] >= 0) ++nnc; else ++npc; }
+    }
+    int tot;
+    const int soff = warp_excl_scan(nnc, lane, tot);
+    if (top + tot > stack_cap) {
+      // capacity exceeded: the group's result is incomplete and flagged;
+      // the host repeats the walk with a larger stack
+      wc.err |= kErrStackOverflow;
+    } else {
+      if (cls == 3) {
+        int k = top + soff;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < mt.w && ch[c] >= 0) stack[k++] = ch[c];
+      }
+      top += tot;
+    }
+    // bodies: lone-particle children (<= 8, one pass) and leaf ranges
+    int rf = 0, rn = 0;
+    if (cls == 2) { rf = mt.x; rn = mt.y; }
+    bool first_pass = true;
+    // nothing to queue on any lane (the common case): no scan
+    for (bool any = __ballot_sync(kFull, rn > 0 || (cls == 3 && npc > 0)) != 0u; any;
+         any = __ballot_sync(kFull, rn > 0) != 0u) {
+      int give;
+      if (first_pass && cls == 3) give = npc;
+      else give = min(rn, kBodyPerLane);
+      int btot;
+      const int boff = warp_excl_scan(give, lane, btot);
+      if (btot == 0) break;
+      if (first_pass && cls == 3) {
+        int k = nbody + boff;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (c < mt.w && ch[c] < 0) bodyq[k++] = ~ch[c];
+      } else {
+        for (int k = 0; k < give; ++k) bodyq[nbody + boff + k] = rf + k;
+        rf += give; rn -= give;
+      }
+      first_pass = false;
+      nbody += btot;
+      __syncwarp();
+      while (nbody >= kWarp) { eval_bodies(nbody, kWarp); nbody -= kWarp; }
+    }
+    __syncwarp();
+    while (ncell >= kWarp) { eval_cells(ncell, kWarp); ncell -= kWarp; }
+    __syncwarp();
+  }
+  if (ncell > 0) eval_cells(ncell, ncell);
+  if (nbody > 0) eval_bodies(nbody, nbody);
+}
+
 // One group: TPL targets per lane (the group has <= 32 * TPL bodies).
 template <typename T, int ORDER, int TPL, bool SOFT>
 __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER> &S,
@@ -386,7 +535,6 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
   constexpr int W = StageWords<ORDER>::value;
   constexpr bool kKahan = sizeof(T) == 4;
   const int lane = threadIdx.x & (kWarp - 1);
-  const unsigned lt = (1u << lane) - 1u;
 
   double px[TPL], py[TPL], pz[TPL];
   bool valid[TPL];
@@ -574,136 +722,8 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
     __syncwarp();
   };
 
-  int top = 1, ncell = 0, nbody = 0;
-  // a tree visits every node at most once per group: more tests than nodes
-  // means a malformed tree, and the walk stops with an error instead of
-  // looping
-  const int64_t max_tests = (int64_t)a.sc->n_compact + kWarp;
-  int64_t group_tests = 0;
-  if (root < 0) top = 0;  // a lone body: no tree, no force
-  if (lane == 0) stack[0] = root;
-  __syncwarp();
-  while (top > 0) {
-    if (group_tests > max_tests) { wc.err |= kErrIndex; break; }
-    const int take = min(top, kWarp);
-    const int base = top - take;
-    const int node = lane < take ? stack[base + lane] : -1;
-    top = base;
-    __syncwarp();
-    int cls = 0;  // 1 cell, 2 open leaf, 3 open internal
-    int4 mt = make_int4(0, 0, 0, 0);
-    T dx = (T)0, dy = (T)0, dz = (T)0, size2 = (T)0;
-    bool cand = false;
-    if (node >= 0) {
-      mt = a.meta[node];
-      const double4 c = a.com[node];
-      dx = (T)((c.x - gc[0]) * inv_s); dy = (T)((c.y - gc[1]) * inv_s); dz = (T)((c.z - gc[2]) * inv_s);
-      const T ex = max(max(blo[0] - dx, (T)0), dx - bhi[0]);
-      const T ey = max(max(blo[1] - dy, (T)0), dy - bhi[1]);
-      const T ez = max(max(blo[2] - dz, (T)0), dz - bhi[2]);
-      const T d2 = fma(ex, ex, fma(ey, ey, ez * ez));
-      size2 = pow2_neg2<T>(mt.z);
-      if (size2 <= theta2 * d2) {
-        cls = 1;
-      } else {
-        cls = (mt.y <= a.leaf_cap || mt.w == 0) ? 2 : 3;
-        if (a.mac == 1 && (mt.x + mt.y <= gf || mt.x >= gf + gn)) {
-          // holds no member: accept when every member passes its own MAC.
-          // Every member is at least |c| - rad from the centre of mass (the
-          // sphere bound); otherwise the members are tested one by one below
-          // if the nearest of them (at most `diag` beyond the box) may pass.
-          const T reach = sqrt(size2 * inv_theta2);
-          const T dc = sqrt(fma(dx, dx, fma(dy, dy, dz * dz)));
-          if (dc - rad >= reach) {
-            cls = 1;
-          } else {
-            const T r2 = reach - diag;
-            cand = r2 <= (T)0 || r2 * r2 <= d2;
-          }
-        }
-      }
-    }
-    // members' own MAC (morton_octree.f90:701-706: size^2 <= theta^2 d^2 with
-    // d from the member to the centre of mass), all members at once
-    for (unsigned pend = __ballot_sync(kFull, cand); pend; pend &= pend - 1) {
-      const int src = __ffs(pend) - 1;
-      const T cx = __shfl_sync(kFull, dx, src), cy = __shfl_sync(kFull, dy, src),
-              cz = __shfl_sync(kFull, dz, src), cs2 = __shfl_sync(kFull, size2, src);
-      T dmin = (T)INFINITY;
-#pragma unroll
-      for (int t = 0; t < TPL; ++t) {
-        const T ux = cx - rx[t], uy = cy - ry[t], uz = cz - rz[t];
-        dmin = min(dmin, fma(ux, ux, fma(uy, uy, uz * uz)));
-      }
-      dmin = warp_min(dmin);
-      if (lane == src && cs2 <= theta2 * dmin) cls = 1;
-    }
-    wc.tests += take;
-    group_tests += take;
-    // cells
-    const unsigned cm = __ballot_sync(kFull, cls == 1);
-    if (cls == 1) S.cellq[ncell + __popc(cm & lt)] = node;
-    ncell += __popc(cm);
-    // children of opened internal nodes
-    int32_t ch[8];
-    int nnc = 0, npc = 0;
-    if (cls == 3) {
-      const int4 *cp = reinterpret_cast<const int4 *>(a.child + 8 * (int64_t)node);
-      const int4 c0 = cp[0], c1 = cp[1];
-      ch[0] = c0.x; ch[1] = c0.y; ch[2] = c0.z; ch[3] = c0.w;
-      ch[4] = c1.x; ch[5] = c1.y; ch[6] = c1.z; ch[7] = c1.w;
-#pragma unroll
-      for (int c = 0; c < 8; ++c)
-        if (c < mt.w) { if (ch[c] >= 0) ++nnc; else ++npc; }
-    }
-    int tot;
-    const int soff = warp_excl_scan(nnc, lane, tot);
-    if (top + tot > stack_cap) {
-      // capacity exceeded: the group's result is incomplete and flagged;
-      // the host repeats the walk with a larger stack
-      wc.err |= kErrStackOverflow;
-    } else {
-      if (cls == 3) {
-        int k = top + soff;
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < mt.w && ch[c] >= 0) stack[k++] = ch[c];
-      }
-      top += tot;
-    }
-    // bodies: lone-particle children (<= 8, one pass) and leaf ranges
-    int rf = 0, rn = 0;
-    if (cls == 2) { rf = mt.x; rn = mt.y; }
-    bool first_pass = true;
-    // nothing to queue on any lane (the common case): no scan
-    for (bool any = __ballot_sync(kFull, rn > 0 || (cls == 3 && npc > 0)) != 0u; any;
-         any = __ballot_sync(kFull, rn > 0) != 0u) {
-      int give;
-      if (first_pass && cls == 3) give = npc;
-      else give = min(rn, kBodyPerLane);
-      int btot;
-      const int boff = warp_excl_scan(give, lane, btot);
-      if (btot == 0) break;
-      if (first_pass && cls == 3) {
-        int k = nbody + boff;
-#pragma unroll
-        for (int c = 0; c < 8; ++c)
-          if (c < mt.w && ch[c] < 0) S.bodyq[k++] = ~ch[c];
-      } else {
-        for (int k = 0; k < give; ++k) S.bodyq[nbody + boff + k] = rf + k;
-        rf += give; rn -= give;
-      }
-      first_pass = false;
-      nbody += btot;
-      __syncwarp();
-      while (nbody >= kWarp) { eval_bodies(nbody, kWarp); nbody -= kWarp; }
-    }
-    __syncwarp();
-    while (ncell >= kWarp) { eval_cells(ncell, kWarp); ncell -= kWarp; }
-    __syncwarp();
-  }
-  if (ncell > 0) eval_cells(ncell, ncell);
-  if (nbody > 0) eval_bodies(nbody, nbody);
+  tree_walk<T, TPL>(a, S.cellq, S.bodyq, stack, stack_cap, gf, gn, root, gc, inv_s, blo, bhi,
+                    theta2, inv_theta2, diag, rad, rx, ry, rz, wc, eval_cells, eval_bodies);
 
   // forces in the original order; every system's result is an (n_s, 3)
   // Fortran-ordered block at 3 * off_s
@@ -756,6 +776,414 @@ group_walk_kernel(WalkArgs a) {
     atomicAdd(&a.stats[0], wc.pp);
     atomicAdd(&a.stats[1], wc.pc);
     atomicAdd(&a.stats[3], wc.tests);
+  }
+}
+
+// ---- warp-specialised FP32 group walk (pipeline = 1) ----
+//
+// A block holds kTeams teams of one producer warp and one consumer warp.
+// The producer takes groups from the global cursor, walks the tree exactly as
+// the one-warp walk does and stages every batch of 32 cells or bodies into a
+// ring of kRing shared-memory slots; its consumer evaluates the batches and
+// writes the forces.  Every target sees the batches of the one-warp walk in
+// the same order with the same arithmetic, so the results are the same bit
+// for bit; the tree walk of one group overlaps the evaluation of another.
+// Producers (warpgroup 0) hand registers to the consumers (warpgroup 1) with
+// setmaxnreg, so that more teams fit on an SM.  Each slot has a "full"
+// mbarrier (32 arrivals: the producer's lanes) and an "empty" one (32
+// arrivals: the consumer's lanes).  Every wait is bounded: a wait that lasts
+// more than about 2 s, or sees the block's abort flag, gives up, sets the flag
+// and reports an error; every warp of the block then leaves its loop.
+
+constexpr int kTeams = 4;
+constexpr int kRing = 4;
+constexpr long long kWaitCycles = 4000000000LL;
+constexpr int kRingStart = 1, kRingCells = 2, kRingBodies = 3, kRingEnd = 4, kRingQuit = 5;
+
+template <int ORDER>
+struct __align__(16) RingSlot {
+  int kind, count, g, unused;
+  double gc[3];
+  double unused2;
+  float stage[kWarp * StageWords<ORDER>::value];
+};
+
+template <int ORDER>
+struct __align__(16) PipeSmem {
+  unsigned long long full[kTeams][kRing];
+  unsigned long long empty[kTeams][kRing];
+  int abort_flag;
+  int cellq[kTeams][kCellQ];
+  int bodyq[kTeams][kBodyQ];
+  RingSlot<ORDER> ring[kTeams][kRing];
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// The whole warp waits for the phase of parity `parity` of barrier b to
+// complete; false when the block was aborted or the wait timed out (which
+// aborts the block).
+__device__ __forceinline__ bool mbar_wait_warp(unsigned long long *b, unsigned parity,
+                                               volatile int *abort_flag) {
+  const long long t0 = clock64();
+  for (;;) {
+    const bool ok = mbar_test(b, parity);
+    if (__all_sync(kFull, ok)) return true;
+    int stop = 0;
+    if ((threadIdx.x & (kWarp - 1)) == 0) {
+      if (*abort_flag) stop = 1;
+      else if (clock64() - t0 > kWaitCycles) { *abort_flag = 1; stop = 1; }
+    }
+    if (__shfl_sync(kFull, stop, 0)) return false;
+  }
+}
+
+// Producer side of one group: the target set-up and tree walk of walk_group,
+// with every batch staged into the ring.  `alive` turns false (for the rest
+// of the kernel) when a wait gave up.
+template <int ORDER, int TPL, bool SOFT>
+__device__ __forceinline__ void produce_group(const WalkArgs &a, PipeSmem<ORDER> &P, int team,
+                                              int &it, bool &alive, volatile int *abort_flag,
+                                              int32_t *stack, int stack_cap, int g, int gf,
+                                              int gn, const SysScalars &ss, float theta2,
+                                              WalkCounters &wc) {
+  using T = float;
+  const double inv_s = 1.0 / ss.ssa, inv_m = 1.0 / ss.mass;
+  const double nq = inv_m * inv_s * inv_s, no = nq * inv_s;
+  constexpr int W = StageWords<ORDER>::value;
+  const int lane = threadIdx.x & (kWarp - 1);
+  double px[TPL], py[TPL], pz[TPL];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    const int k = lane + kWarp * t;
+    const double4 p = a.spos[gf + (k < gn ? k : 0)];
+    px[t] = p.x; py[t] = p.y; pz[t] = p.z;
+  }
+  double lo[3] = {px[0], py[0], pz[0]}, hi[3] = {px[0], py[0], pz[0]};
+#pragma unroll
+  for (int t = 1; t < TPL; ++t) {
+    lo[0] = fmin(lo[0], px[t]); hi[0] = fmax(hi[0], px[t]);
+    lo[1] = fmin(lo[1], py[t]); hi[1] = fmax(hi[1], py[t]);
+    lo[2] = fmin(lo[2], pz[t]); hi[2] = fmax(hi[2], pz[t]);
+  }
+  double gc[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) gc[k] = 0.5 * (warp_min(lo[k]) + warp_max(hi[k]));
+  T rx[TPL], ry[TPL], rz[TPL], blo[3], bhi[3];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    rx[t] = (T)((px[t] - gc[0]) * inv_s);
+    ry[t] = (T)((py[t] - gc[1]) * inv_s);
+    rz[t] = (T)((pz[t] - gc[2]) * inv_s);
+    if (t == 0) { blo[0] = bhi[0] = rx[0]; blo[1] = bhi[1] = ry[0]; blo[2] = bhi[2] = rz[0]; }
+    else {
+      blo[0] = min(blo[0], rx[t]); bhi[0] = max(bhi[0], rx[t]);
+      blo[1] = min(blo[1], ry[t]); bhi[1] = max(bhi[1], ry[t]);
+      blo[2] = min(blo[2], rz[t]); bhi[2] = max(bhi[2], rz[t]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { blo[k] = warp_min(blo[k]); bhi[k] = warp_max(bhi[k]); }
+  const T diag = sqrt((bhi[0] - blo[0]) * (bhi[0] - blo[0]) + (bhi[1] - blo[1]) * (bhi[1] - blo[1]) +
+                      (bhi[2] - blo[2]) * (bhi[2] - blo[2]));
+  const T inv_theta2 = theta2 > (T)0 ? (T)1 / theta2 : (T)INFINITY;
+  T rad2 = (T)0;
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) rad2 = max(rad2, fma(rx[t], rx[t], fma(ry[t], ry[t], rz[t] * rz[t])));
+  const T rad = sqrt(warp_max(rad2));
+
+  // the next slot, once its consumer has released it
+  auto acquire = [&]() -> RingSlot<ORDER> * {
+    const int slot = it % kRing;
+    const unsigned round = (unsigned)(it / kRing);
+    if (alive && round > 0 && !mbar_wait_warp(&P.empty[team][slot], (round - 1) & 1u, abort_flag))
+      alive = false;
+    return &P.ring[team][slot];
+  };
+  auto publish = [&]() {
+    __syncwarp();
+    mbar_arrive(&P.full[team][it % kRing]);
+    ++it;
+  };
+  RingSlot<ORDER> *R = acquire();
+  if (alive) {
+    if (lane == 0) {
+      R->kind = kRingStart; R->g = g; R->count = gn;
+      R->gc[0] = gc[0]; R->gc[1] = gc[1]; R->gc[2] = gc[2];
+    }
+    publish();
+  }
+  // the stage layouts of walk_group's paired evaluation
+  auto emit_cells = [&](int end, int nc) {
+    RingSlot<ORDER> *Q = acquire();
+    if (!alive) return;
+    float *w = Q->stage + (lane >> 1) * 2 * W + (lane & 1);
+    if (lane < nc) {
+      stage_cell<float, ORDER, 2>(w, P.cellq[team][end - nc + lane], a, gc, inv_s, inv_m, nq, no);
+    } else if (lane == nc && (nc & 1)) {
+#pragma unroll
+      for (int k = 3; k < W; ++k) w[2 * k] = 0.0f;
+      w[0] = w[2] = w[4] = kPadPos;
+    }
+    if (lane == 0) { Q->kind = kRingCells; Q->count = nc; }
+    wc.pc += (unsigned long long)nc * gn;
+    publish();
+  };
+  auto emit_bodies = [&](int end, int nb) {
+    RingSlot<ORDER> *Q = acquire();
+    if (!alive) return;
+    float *w = Q->stage + (lane >> 1) * 8 + (lane & 1);
+    if (lane < nb) {
+      const int p = P.bodyq[team][end - nb + lane];
+      const double4 sp = a.spos[p];
+      w[0] = (float)((sp.x - gc[0]) * inv_s);
+      w[2] = (float)((sp.y - gc[1]) * inv_s);
+      w[4] = (float)((sp.z - gc[2]) * inv_s);
+      w[6] = (float)(sp.w * inv_m);
+    } else if (lane == nb && (nb & 1)) {
+      w[0] = w[2] = w[4] = kPadPos;
+      w[6] = 0.0f;
+    }
+    if (lane == 0) { Q->kind = kRingBodies; Q->count = nb; }
+    wc.pp += (unsigned long long)nb * gn;
+    publish();
+  };
+  tree_walk<T, TPL>(a, P.cellq[team], P.bodyq[team], stack, stack_cap, gf, gn, ss.root, gc, inv_s,
+                    blo, bhi, theta2, inv_theta2, diag, rad, rx, ry, rz, wc, emit_cells,
+                    emit_bodies);
+  R = acquire();
+  if (alive) {
+    if (lane == 0) R->kind = kRingEnd;
+    publish();
+  }
+}
+
+// Consumer side of one group (its start slot already read and released):
+// evaluates batches until the group's end slot, then writes the forces as
+// walk_group does; false when a wait gave up.
+template <int ORDER, int TPL, bool SOFT>
+__device__ __forceinline__ bool consume_group(const WalkArgs &a, PipeSmem<ORDER> &P, int team,
+                                              int &it, volatile int *abort_flag, int gf, int gn,
+                                              const double gc[3], const SysScalars &ss) {
+  using T = float;
+  constexpr int W = StageWords<ORDER>::value;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const double inv_s = 1.0 / ss.ssa;
+  const T eps2 = (T)(a.eps2 * inv_s * inv_s);
+  const float2 eps2p = splat(eps2);
+  bool valid[TPL];
+  float2 nrx[TPL], nry[TPL], nrz[TPL];
+  T ax[TPL], ay[TPL], az[TPL], cx[TPL], cy[TPL], cz[TPL];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    const int k = lane + kWarp * t;
+    valid[t] = k < gn;
+    const double4 p = a.spos[gf + (valid[t] ? k : 0)];
+    nrx[t] = splat(-(T)((p.x - gc[0]) * inv_s));
+    nry[t] = splat(-(T)((p.y - gc[1]) * inv_s));
+    nrz[t] = splat(-(T)((p.z - gc[2]) * inv_s));
+    ax[t] = ay[t] = az[t] = cx[t] = cy[t] = cz[t] = (T)0;
+  }
+  for (;;) {
+    const int slot = it % kRing;
+    const unsigned round = (unsigned)(it / kRing);
+    if (!mbar_wait_warp(&P.full[team][slot], round & 1u, abort_flag)) return false;
+    const RingSlot<ORDER> &R = P.ring[team][slot];
+    const int kind = R.kind, cnt = R.count;
+    if (kind == kRingCells) {
+      float2 bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = make_float2(0.0f, 0.0f);
+      const int np = (cnt + 1) >> 1;
+#pragma unroll 2
+      for (int j = 0; j < np; ++j) {
+        const float4 *st = reinterpret_cast<const float4 *>(R.stage) + j * (W / 2);
+        float2 cw[W];
+#pragma unroll
+        for (int k = 0; k < W / 2; ++k) {
+          const float4 v = st[k];
+          cw[2 * k] = make_float2(v.x, v.y);
+          cw[2 * k + 1] = make_float2(v.z, v.w);
+        }
+#pragma unroll
+        for (int t = 0; t < TPL; ++t)
+          cell_force2<ORDER>(cw, nrx[t], nry[t], nrz[t], eps2p, bx[t], by[t], bz[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        kahan_add(ax[t], cx[t], bx[t].x + bx[t].y);
+        kahan_add(ay[t], cy[t], by[t].x + by[t].y);
+        kahan_add(az[t], cz[t], bz[t].x + bz[t].y);
+      }
+    } else if (kind == kRingBodies) {
+      float2 bx[TPL], by[TPL], bz[TPL];
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) bx[t] = by[t] = bz[t] = make_float2(0.0f, 0.0f);
+      const int np = (cnt + 1) >> 1;
+      const float4 *st = reinterpret_cast<const float4 *>(R.stage);
+      for (int j = 0; j < np; ++j) {
+        const float4 u = st[2 * j], v = st[2 * j + 1];
+        const float2 sx = make_float2(u.x, u.y), sy = make_float2(u.z, u.w);
+        const float2 sz = make_float2(v.x, v.y), sm = make_float2(v.z, v.w);
+#pragma unroll
+        for (int t = 0; t < TPL; ++t)
+          body_force2<SOFT>(sx, sy, sz, sm, nrx[t], nry[t], nrz[t], eps2p, bx[t], by[t], bz[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        kahan_add(ax[t], cx[t], bx[t].x + bx[t].y);
+        kahan_add(ay[t], cy[t], by[t].x + by[t].y);
+        kahan_add(az[t], cz[t], bz[t].x + bz[t].y);
+      }
+    }
+    __syncwarp();
+    mbar_arrive(&P.empty[team][slot]);
+    ++it;
+    if (kind == kRingEnd) break;
+  }
+  const double scale = a.G * ss.mass * inv_s * inv_s;
+  double *out = a.out + 3 * ss.off;
+  const int64_t ns = ss.n;
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    if (!valid[t]) continue;
+    const int i = gf + lane + kWarp * t;
+    const int64_t p = a.perm[i] - ss.off;
+    double fxs = (double)ax[t], fys = (double)ay[t], fzs = (double)az[t];
+    fxs -= (double)cx[t]; fys -= (double)cy[t]; fzs -= (double)cz[t];
+    double sc = scale;
+    if (a.out_kind == 0) sc *= a.spos[i].w;
+    out[p] = fxs * sc;
+    out[ns + p] = fys * sc;
+    out[2 * ns + p] = fzs * sc;
+  }
+  return true;
+}
+
+// PipeRegs<ORDER>::blocks blocks of 2 kTeams warps per SM.  At launch every
+// thread holds `regs` registers (the most that `blocks` blocks allow); the
+// producer warpgroup then gives registers up to the consumer warpgroup:
+// producer + consumer = 2 regs, so the consumers' request is always covered by
+// the block's own registers (the host checks the launch count first).  The
+// quadrupole consumer runs without spills at 96, the octupole one needs more.
+constexpr int kPipeThreads = 2 * kTeams * kWarp;
+static_assert(kTeams == 4, "one warpgroup of producers, one of consumers");
+template <int ORDER> struct PipeRegs {
+  static constexpr int blocks = ORDER >= 8 ? 2 : 3;
+  static constexpr int regs = ORDER >= 8 ? 128 : 80;
+  static constexpr int producer = ORDER >= 8 ? 96 : 64;
+  static constexpr int consumer = 2 * regs - producer;
+  static_assert(regs * kPipeThreads * blocks <= 65536, "register file");
+  static_assert(regs % 8 == 0 && producer % 8 == 0 && consumer <= 256, "setmaxnreg counts");
+};
+
+template <int ORDER, int MAXTPL, bool SOFT>
+__global__ void __launch_bounds__(kPipeThreads, PipeRegs<ORDER>::blocks)
+pipe_walk_kernel(WalkArgs a) {
+  extern __shared__ __align__(16) unsigned char pipe_smem_raw[];
+  PipeSmem<ORDER> &P = *reinterpret_cast<PipeSmem<ORDER> *>(pipe_smem_raw);
+  const int warp = threadIdx.x / kWarp, lane = threadIdx.x & (kWarp - 1);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kTeams; ++q)
+      for (int r = 0; r < kRing; ++r) {
+        mbar_init(&P.full[q][r], kWarp);
+        mbar_init(&P.empty[q][r], kWarp);
+      }
+    P.abort_flag = 0;
+  }
+  __syncthreads();
+  volatile int *abort_flag = &P.abort_flag;
+  const int ngroups = a.g_end >= 0 ? min(a.g_end, a.sc->n_groups) : a.sc->n_groups;
+  int it = 0;
+  if (warp < kTeams) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(PipeRegs<ORDER>::producer));
+    const int team = warp;
+    int32_t *stack = a.stack + ((int64_t)blockIdx.x * kTeams + team) * a.stack_cap;
+    const int stack_cap = (int)a.stack_cap;
+    const float theta2 = (float)a.theta2;
+    WalkCounters wc;
+    bool alive = true;
+    for (;;) {
+      int g = 0;
+      if (lane == 0) g = a.g_begin + atomicAdd(a.cursor, 1);
+      g = __shfl_sync(kFull, g, 0);
+      if (g >= ngroups) break;
+      const int gf = a.g_first[g];
+      const int gn = a.g_first[g + 1] - gf;
+      const SysScalars &ss = a.ss[a.sys_of[gf]];
+      if (MAXTPL == 2 && gn > kWarp)
+        produce_group<ORDER, 2, SOFT>(a, P, team, it, alive, abort_flag, stack, stack_cap, g, gf,
+                                      gn, ss, theta2, wc);
+      else
+        produce_group<ORDER, 1, SOFT>(a, P, team, it, alive, abort_flag, stack, stack_cap, g, gf,
+                                      gn, ss, theta2, wc);
+      if (!alive) break;
+    }
+    if (alive) {  // tell the consumer there is nothing more
+      const int slot = it % kRing;
+      const unsigned round = (unsigned)(it / kRing);
+      if (round == 0 || mbar_wait_warp(&P.empty[team][slot], (round - 1) & 1u, abort_flag)) {
+        if (lane == 0) P.ring[team][slot].kind = kRingQuit;
+        __syncwarp();
+        mbar_arrive(&P.full[team][slot]);
+      }
+    }
+    if (lane == 0) {
+      if (wc.err) atomicOr(&a.sc->err, wc.err);
+      if (!alive) atomicOr(&a.sc->err, kErrTimeout);
+      if (a.count_stats) {
+        atomicAdd(&a.stats[0], wc.pp);
+        atomicAdd(&a.stats[1], wc.pc);
+        atomicAdd(&a.stats[3], wc.tests);
+      }
+    }
+  } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(PipeRegs<ORDER>::consumer));
+    const int team = warp - kTeams;
+    for (;;) {
+      const int slot = it % kRing;
+      const unsigned round = (unsigned)(it / kRing);
+      if (!mbar_wait_warp(&P.full[team][slot], round & 1u, abort_flag)) {
+        if (lane == 0) atomicOr(&a.sc->err, kErrTimeout);
+        break;
+      }
+      const RingSlot<ORDER> &R = P.ring[team][slot];
+      const int kind = R.kind, g = R.g, gn = R.count;
+      const double gc[3] = {R.gc[0], R.gc[1], R.gc[2]};
+      __syncwarp();
+      mbar_arrive(&P.empty[team][slot]);
+      ++it;
+      if (kind != kRingStart) break;  // the producer has no more groups
+      const int gf = a.g_first[g];
+      const SysScalars &ss = a.ss[a.sys_of[gf]];
+      bool ok;
+      if (MAXTPL == 2 && gn > kWarp)
+        ok = consume_group<ORDER, 2, SOFT>(a, P, team, it, abort_flag, gf, gn, gc, ss);
+      else
+        ok = consume_group<ORDER, 1, SOFT>(a, P, team, it, abort_flag, gf, gn, gc, ss);
+      if (!ok) {
+        if (lane == 0) atomicOr(&a.sc->err, kErrTimeout);
+        break;
+      }
+    }
   }
 }
 
@@ -931,8 +1359,38 @@ int sm_count() {
 // instantiation)
 int64_t walk_slots() { return (int64_t)sm_count() * kWalkBlocksPerSm; }
 
+// The pipelined walk, when the kernel was built with the register count its
+// setmaxnreg split assumes; returns false (nothing launched) otherwise.
+template <int ORDER, int MAXTPL, bool SOFT>
+static bool launch_pipe_walk(const WalkArgs &a, cudaStream_t s) {
+  // the shared-memory limit is a per-device attribute: set it once per device
+  static int per_sm[64] = {};
+  const int smem = (int)sizeof(PipeSmem<ORDER>);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (per_sm[dev] == 0) {
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, pipe_walk_kernel<ORDER, MAXTPL, SOFT>);
+    cudaFuncSetAttribute(pipe_walk_kernel<ORDER, MAXTPL, SOFT>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int v = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, pipe_walk_kernel<ORDER, MAXTPL, SOFT>,
+                                                  kPipeThreads, smem);
+    // a block launched with fewer registers than the split hands out would
+    // wait for ever in setmaxnreg.inc: never launch it
+    per_sm[dev] = (fa.numRegs == PipeRegs<ORDER>::regs && v > 0) ? v : -1;
+  }
+  if (per_sm[dev] < 0) return false;
+  int64_t blocks = (int64_t)per_sm[dev] * sm_count();
+  if (blocks * kTeams > a.slots) blocks = a.slots / kTeams;  // one stack per producer
+  pipe_walk_kernel<ORDER, MAXTPL, SOFT><<<(unsigned)blocks, kPipeThreads, smem, s>>>(a);
+  return true;
+}
+
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
 static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
+  if (sizeof(T) == 4 && a.pipeline && launch_pipe_walk<ORDER, MAXTPL, SOFT>(a, s)) return;
   // exactly the blocks that are resident at once: no block waits for a
   // second wave behind the walk (which would also hold back other streams)
   static int per_sm = 0;
@@ -959,6 +1417,7 @@ static WalkArgs make_args(int64_t n, const WalkParams &p, Buffers &b, double *ou
   a.out_kind = p.out_kind; a.leaf_cap = p.leaf_cap; a.count_stats = p.count_stats;
   a.mac = p.mac;
   a.g_begin = p.g_begin; a.g_end = p.g_end;
+  a.pipeline = p.pipeline;
   return a;
 }
 

@@ -68,12 +68,15 @@ typedef struct bh_params {
                          (octree_default.f90:1927-1936); 1 also accept a node that
                          fails it when it holds none of the group's bodies and passes
                          every group member's own MAC (morton_octree.f90:701-706)   */
-    int reserved[1];
+    int pipeline;     /* FP32 group walk: 0 one warp walks a group and evaluates it;
+                         1 producer warps walk the tree and stage the batches into a
+                         shared-memory ring, consumer warps evaluate them (the same
+                         results bit for bit; no reference counterpart)            */
 } bh_params;
 
 /* Defaults: theta 0.5, G 1, eps 0, order 4, forces, depth 21, FP32, amp 1.2,
  * group 64, leaf_cap 8, com_mode 1, strict_keys 1, count_stats 0, group_span 0,
- * mac 0. */
+ * mac 0, pipeline 0. */
 void bh_params_default(bh_params *p);
 
 const char *bh_version(void);

@@ -57,7 +57,7 @@ def test_params_struct_layout_matches_c(built_lib):
 int main(void) {
   printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(bh_params), offsetof(bh_params, amp),
          offsetof(bh_params, group_size), offsetof(bh_params, strict_keys),
-         offsetof(bh_params, reserved), offsetof(bh_params, precision), offsetof(bh_params, order));
+         offsetof(bh_params, pipeline), offsetof(bh_params, precision), offsetof(bh_params, order));
   return 0;
 }
 '''
@@ -70,7 +70,7 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
         vals = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     mine = [C.sizeof(BHParams), BHParams.amp.offset, BHParams.group_size.offset,
-            BHParams.strict_keys.offset, BHParams.reserved.offset, BHParams.precision.offset,
+            BHParams.strict_keys.offset, BHParams.pipeline.offset, BHParams.precision.offset,
             BHParams.order.offset]
     assert vals == mine
 
