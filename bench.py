@@ -73,10 +73,12 @@ def parse():
     ap.add_argument("--group-size", type=int, default=64)
     ap.add_argument("--leaf-cap", type=int, default=8)
     ap.add_argument("--group-span", type=int, default=0)
-    ap.add_argument("--mac", type=int, default=None,
-                    help="group walk acceptance: 0 box distance, 1 box or every member's own MAC")
+    ap.add_argument("--mac", type=int, default=1,
+                    help="group walk acceptance: 0 the group's box distance, 1 also a node that "
+                         "every member's own MAC accepts (default)")
     ap.add_argument("--pipeline", type=int, default=None,
-                    help="FP32 walk: 0 one warp per group, 1 producer/consumer warp teams")
+                    help="FP32 walk: 0 one warp per group, 1 producer/consumer warp teams "
+                         "(the library default)")
     ap.add_argument("--lanes", type=int, default=2)
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--split-system", action="store_true",
@@ -405,7 +407,9 @@ def run_ours(args):
             with open(tf) as fh:
                 traffic = json.load(fh).get("bytes_per_launch_scaled")
         line["roofline"] = {
-            "bound": "fp32", "kernel": "group_walk_kernel", "achieved": achieved,
+            "bound": "fp32",
+            "kernel": "pipe_walk_kernel" if p.pipeline and args.precision == 0 else "group_walk_kernel",
+            "achieved": achieved,
             "peak": fp32_peak / 1e3, "unit": "TFLOP/s", "frac": achieved / (fp32_peak / 1e3),
             "traffic": traffic,
             "peak_source": "FP32 FMA throughput measured by bh_probe_fma_peak in this run, the larger "
