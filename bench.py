@@ -55,8 +55,27 @@ import numpy as np  # noqa: E402
 N_DEFAULT = 1 << 20
 THETA, EPS, ORDER = 0.5, 0.01, 4
 N_ERR_TARGETS = 16384
-FLOPS_PP = 20          # body-body (GPU Gems 3 convention), morton_octree.f90:676-686
-FLOPS_PC = {1: 20, 4: 60, 8: 140}  # cell terms, octree_default.f90:1993-2083
+# Algorithmic flops per interaction, each operation of the reference's formulas
+# listed once (a multiply-add counts 2; in the body-body term rsqrt counts 2,
+# which gives the usual 20 of the GPU Gems 3 convention).
+FLOP_OPS = {
+    # morton_octree.f90:676-686 (and the monopole cell term :711-718)
+    "body_body": [("d = x_j - x_i", 3), ("r2 = d.d + eps2", 6), ("rsqrt", 2),
+                  ("r^-3 = rinv^3", 2), ("m r^-3", 1), ("a += s d", 6)],
+    # octree_default.f90:2009-2027 (a10's quadrupole cell term; rsqrt counts 1 here)
+    "quad_cell": [("d = c - x_i", 3), ("r2 = d.d + eps2", 6), ("rsqrt", 1),
+                  ("powers r^-2 .. r^-7", 6), ("Q d (3 rows of 3 terms)", 15), ("d.Q.d", 5),
+                  ("1.5 trQ", 2), ("s = M/r^3 - 1.5 trQ/r^5 + 7.5 dQd/r^7", 7),
+                  ("a += s d - 3 Q d / r^5", 15)],
+    # octree_default.f90:2033-2082 (a10's octupole cell term, on top of the quadrupole)
+    "oct_extra": [("r^-4 and the 7.5, -1.5, -17.5 prefactors", 5), ("pair products of d", 6),
+                  ("O_{12..14}.d and its scale", 6), ("three rows of O contracted with d d", 42),
+                  ("cubic contraction O:ddd", 17), ("a += r^-3 o", 4)],
+}
+FLOPS_PP = sum(k for _, k in FLOP_OPS["body_body"])                 # 20
+_QUAD = sum(k for _, k in FLOP_OPS["quad_cell"])                    # 60
+FLOPS_PC = {1: FLOPS_PP, 4: _QUAD, 8: _QUAD + sum(k for _, k in FLOP_OPS["oct_extra"])}
+assert (FLOPS_PP, FLOPS_PC[4], FLOPS_PC[8]) == (20, 60, 140)
 METRIC = "forces/s (N=1M, theta=0.5, err<=1e-3 vs FP64): served vs plain; p50/p99 ms"
 
 
