@@ -36,7 +36,7 @@ EXPORTED = [
     "bh_system_walk_groups",
     "bh_system_forces", "bh_system_sync", "bh_system_info", "bh_system_get_keys",
     "bh_system_get_nodes", "bh_system_get_groups", "bh_system_get_stats",
-    "bh_system_reference_targets", "bh_probe_fma_peak", "bh_compute_forces_noalloc",
+    "bh_system_reference_targets", "bh_probe_fma_peak", "bh_probe_bounded_wait", "bh_compute_forces_noalloc",
     "bh_system_build_batch", "bh_system_forces_batch", "bh_system_batch_info",
     "bh_system_capture", "bh_system_replay", "bh_kick_drift", "bh_diagnostics",
     "bh_kick_drift_systems", "bh_generate_ics", "bh_system_reserve",
@@ -108,6 +108,7 @@ def lib():
             "bh_system_get_stats": [_vp, _vp],
             "bh_system_reference_targets": [_vp, C.POINTER(BHParams), _vp, _i64, _vp, _vp, _vp],
             "bh_probe_fma_peak": [_i, _vp],
+            "bh_probe_bounded_wait": [_i, C.c_longlong, _vp],
             "bh_compute_forces_noalloc": [_vp, _vp, _vp, _vp, _i64, C.POINTER(BHParams), _vp, _vp],
             "bh_system_build_batch": [_vp, _vp, _vp, _vp, _vp, _vp, _i, C.POINTER(BHParams), _vp],
             "bh_system_forces_batch": [_vp, _vp, _vp, _vp, _vp, _vp, _i, C.POINTER(BHParams), _vp,

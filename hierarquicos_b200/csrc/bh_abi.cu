@@ -854,6 +854,15 @@ int bh_direct_targets_device(const double *d_m, const double *d_x, const double 
   return BH_OK;
 }
 
+int bh_probe_bounded_wait(int device, long long cycles, long long *out5) {
+  if (!out5) return set_err(BH_ERR_INVALID, "NULL output");
+  if (cycles < 1000 || cycles > 1000000000LL)
+    return set_err(BH_ERR_INVALID, "cycles must be in [1e3, 1e9]");
+  BH_CUDA(cudaSetDevice(device));
+  if (bh::probe_bounded_wait(cycles, out5)) return set_err(BH_ERR_CUDA, "wait probe failed");
+  return BH_OK;
+}
+
 int bh_probe_fma_peak(int device, double *gflops2) {
   if (!gflops2) return set_err(BH_ERR_INVALID, "NULL output");
   BH_CUDA(cudaSetDevice(device));

@@ -169,6 +169,10 @@ void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s);
 void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s);
 void launch_groups(int64_t n, int group_size, int group_span, Buffers &b, cudaStream_t s);
 
+// Runs the check of the pipelined walk's bounded mbarrier waits (one block
+// of two warps; `cycles` is the short limit); out5 as in wait_probe_kernel.
+int probe_bounded_wait(long long cycles, long long *out5);
+
 struct WalkParams {
   double theta2, G, eps2;
   int order;       // 1, 4, 8

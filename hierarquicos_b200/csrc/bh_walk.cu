@@ -839,10 +839,11 @@ __device__ __forceinline__ bool mbar_test(unsigned long long *b, unsigned parity
   return ok != 0;
 }
 // The whole warp waits for the phase of parity `parity` of barrier b to
-// complete; false when the block was aborted or the wait timed out (which
-// aborts the block).
+// complete; false when the block was aborted or the wait lasted more than
+// `limit` cycles (which aborts the block).
 __device__ __forceinline__ bool mbar_wait_warp(unsigned long long *b, unsigned parity,
-                                               volatile int *abort_flag) {
+                                               volatile int *abort_flag,
+                                               long long limit = kWaitCycles) {
   const long long t0 = clock64();
   for (;;) {
     const bool ok = mbar_test(b, parity);
@@ -850,7 +851,7 @@ __device__ __forceinline__ bool mbar_wait_warp(unsigned long long *b, unsigned p
     int stop = 0;
     if ((threadIdx.x & (kWarp - 1)) == 0) {
       if (*abort_flag) stop = 1;
-      else if (clock64() - t0 > kWaitCycles) { *abort_flag = 1; stop = 1; }
+      else if (clock64() - t0 > limit) { *abort_flag = 1; stop = 1; }
     }
     if (__shfl_sync(kFull, stop, 0)) return false;
   }
@@ -1187,6 +1188,42 @@ pipe_walk_kernel(WalkArgs a) {
   }
 }
 
+// Check of the bounded waits above on one block of two warps.  Warp 0 arrives
+// at barrier 2 (a phase that completes), waits until warp 1 has seen it
+// complete, then waits on barrier 0, at which nothing ever arrives, for
+// `limit` cycles.  Warp 1 waits on barrier 2, acknowledges on barrier 1, then
+// waits on barrier 0 with the walk's full limit: it must be released by the
+// abort flag that warp 0 sets when it gives up.  out: [0] warp 0's result on
+// barrier 0, [1] warp 1's result on barrier 2, [2] warp 1's result on barrier
+// 0, [3] the cycles warp 1 waited there, [4] the abort flag at the end.
+__global__ void __launch_bounds__(2 * kWarp) wait_probe_kernel(long long limit, long long *out) {
+  __shared__ __align__(8) unsigned long long bar[3];
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x / kWarp, lane = threadIdx.x & (kWarp - 1);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 3; ++k) mbar_init(&bar[k], kWarp);
+    abort_flag = 0;
+  }
+  __syncthreads();
+  volatile int *af = &abort_flag;
+  if (warp == 0) {
+    mbar_arrive(&bar[2]);
+    const bool acked = mbar_wait_warp(&bar[1], 0, af, limit);
+    const bool ok = acked && mbar_wait_warp(&bar[0], 0, af, limit);
+    if (lane == 0) out[0] = ok ? 1 : 0;
+  } else {
+    const bool seen = mbar_wait_warp(&bar[2], 0, af, limit);
+    if (lane == 0) out[1] = seen ? 1 : 0;
+    mbar_arrive(&bar[1]);
+    const long long t0 = clock64();
+    const bool ok = mbar_wait_warp(&bar[0], 0, af);
+    const long long dt = clock64() - t0;
+    if (lane == 0) { out[2] = ok ? 1 : 0; out[3] = dt; }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) out[4] = abort_flag;
+}
+
 // ---- reference-semantics walk (FP64, one thread per target) ----
 
 __device__ __forceinline__ void ref_pp(double bx, double by, double bz, double bm, double qp0,
@@ -1358,6 +1395,21 @@ int sm_count() {
 // stack slots: one per resident walk block of the FP32 walk (the most of any
 // instantiation)
 int64_t walk_slots() { return (int64_t)sm_count() * kWalkBlocksPerSm; }
+
+int probe_bounded_wait(long long cycles, long long *out5) {
+  long long *d = nullptr;
+  if (cudaMalloc(&d, 5 * sizeof(long long)) != cudaSuccess) return 1;
+  int rc = 0;
+  if (cudaMemset(d, 0xff, 5 * sizeof(long long)) != cudaSuccess) rc = 1;
+  if (!rc) {
+    wait_probe_kernel<<<1, 2 * kWarp>>>(cycles, d);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = 1;
+  }
+  if (!rc && cudaMemcpy(out5, d, 5 * sizeof(long long), cudaMemcpyDeviceToHost) != cudaSuccess)
+    rc = 1;
+  cudaFree(d);
+  return rc;
+}
 
 // The pipelined walk, when the kernel was built with the register count its
 // setmaxnreg split assumes; returns false (nothing launched) otherwise.

@@ -274,6 +274,16 @@ int bh_generate_ics(int profile, int64_t n, double size_qs, double size_ps, int 
  * (FP32 issued as paired f32x2 instructions); gflops2 holds 3 doubles. */
 int bh_probe_fma_peak(int device, double *gflops2);
 
+/* Check of the bounded waits of the pipelined walk (no reference counterpart):
+ * one block of two warps uses the walk's mbarrier wait.  Warp 0 waits
+ * `cycles` clock cycles (1e3..1e9) on a barrier nothing arrives at, gives up
+ * and raises the block's abort flag; warp 1, waiting on the same barrier with
+ * the walk's own limit (about 2 s), must be released by that flag.  out5:
+ * [0] warp 0's result (0 = gave up), [1] 1 when a barrier phase that does
+ * complete was seen, [2] warp 1's result (0 = released), [3] the cycles warp 1
+ * waited, [4] the abort flag (1).  Synchronous; allocates 40 bytes. */
+int bh_probe_bounded_wait(int device, long long cycles, long long *out5);
+
 #ifdef __cplusplus
 }
 #endif

@@ -128,3 +128,25 @@ def test_pipeline_large(bh):
     f0, f1, st0, st1 = both(s, order=4, group_size=64, eps=0.01, theta=0.5)
     assert torch.equal(f0, f1)
     np.testing.assert_array_equal(st0[:2], st1[:2])
+
+
+def test_bounded_wait_gives_up_and_releases_the_block(bh):
+    """The walk's mbarrier wait on a barrier that nothing arrives at gives up
+    after its limit, raises the block's abort flag, and that flag releases the
+    other warp of the block long before its own (about 2 s) limit; afterwards
+    the context still runs the force pipeline."""
+    import ctypes as C
+
+    import torch
+    from hierarquicos_b200._lib import check, lib
+
+    limit = 2_000_000
+    out = (C.c_longlong * 5)()
+    check(lib().bh_probe_bounded_wait(torch.cuda.current_device(), limit, out))
+    gave_up, seen, released, waited, flag = list(out)
+    assert seen == 1 and gave_up == 0 and released == 0 and flag == 1
+    assert 0 < waited < 100 * limit
+    m, q = plummer(3000, seed=2)
+    f = bh.BHSystem().forces(m, *xyz(q), eps=0.01)
+    torch.cuda.synchronize()
+    assert torch.isfinite(f).all()
