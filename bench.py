@@ -103,6 +103,11 @@ def parse():
     ap.add_argument("--split-system", action="store_true",
                     help="strong scaling: every rank takes the same system and walks its share of "
                          "the target groups; one all-reduce combines them (implies --no-extras)")
+    ap.add_argument("--serving-sweep", action="store_true",
+                    help="instead of the headline line: the serving config (Poisson arrivals, "
+                         "rate swept, force and leapfrog requests, N log-uniform in [1024, 2^21] "
+                         "over three profiles); prints one JSON line of its own")
+    ap.add_argument("--sweep-requests", type=int, default=48)
     ap.add_argument("--no-extras", action="store_true",
                     help="plain timed calls only (no serving, error check, e2e, batch or CPU baseline)")
     return ap.parse_args()
@@ -719,10 +724,92 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serving_sweep(args):
+    """The serving config: a seeded request set (force or leapfrog with equal
+    odds, 1-100 steps of dt = 1e-3, N log-uniform in [1024, 2^21], Plummer /
+    Hernquist / uniform sphere in turn, device-resident, theta 0.5 quadrupole,
+    150 GB admission budget).  First the set is submitted at once (capacity:
+    requests/s and forces/s); then it arrives as a Poisson stream at fractions
+    of that capacity.  Per rate: p50/p99 latency (arrival to result) and
+    forces/s over the run."""
+    import torch
+
+    from hierarquicos_b200 import _lib, serving
+    from hierarquicos_b200.initial_values import generate_initial_values_device
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(local)
+    p = _lib.default_params(theta=THETA, eps=EPS, order=args.order, mac=args.mac)
+    if args.pipeline is not None:
+        p.pipeline = args.pipeline
+    rng = np.random.default_rng(2026)
+    profiles = ("plummer", "hernquist", "homogeneous")
+    specs = []
+    for i in range(args.sweep_requests):
+        n = int(np.exp(rng.uniform(np.log(1024), np.log(1 << 21))))
+        leap = bool(rng.random() < 0.5)
+        steps = int(rng.integers(1, 101)) if leap else 0
+        m, q, mom = generate_initial_values_device(
+            n, 100.0 if profiles[i % 3] == "hernquist" else -1.0, -1.0, True, False,
+            profiles[i % 3], (1.0, 1.0), seed=5000 + i, velocities=leap, device=local)
+        specs.append((m, q, mom if leap else None, steps))
+    torch.cuda.synchronize()
+
+    def requests():
+        return [serving.Request("leapfrog", m, q, mom, steps=st, dt=1e-3) if st
+                else serving.Request("force", m, q) for m, q, mom, st in specs]
+
+    def run(reqs, rate=None):
+        with serving.Server(p, device=local, lanes=args.lanes, hbm_budget=150e9) as srv:
+            warm = sorted(requests(), key=lambda r: r.n * r.evals_needed)[:3]
+            for r in warm:                                # warm-up: the 3 smallest
+                srv.submit(r)
+            srv.drain(timeout=1200)
+            t0 = time.perf_counter()
+            gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
+            t_next = t0
+            for r, g in zip(reqs, gaps):
+                t_next += g
+                delay = t_next - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                r.arrival = time.perf_counter()
+                srv.submit(r)
+            srv.drain(timeout=1200)
+            torch.cuda.synchronize()
+            return srv.metrics(reqs)
+
+    cap = run(requests())
+    cap_rps = cap["requests"] / cap["wall_s"]
+    rates = []
+    for load in (0.5, 0.8, 0.95):
+        met = run(requests(), rate=load * cap_rps)
+        rates.append({"load": load, "rate_rps": load * cap_rps, "p50_ms": met["p50_ms"],
+                      "p99_ms": met["p99_ms"], "forces_per_s": met["forces_per_s"],
+                      "wall_s": met["wall_s"], "requests": met["requests"]})
+    sizes = [int(sp[0].numel()) for sp in specs]
+    print(json.dumps({
+        "metric": "serving: Poisson arrivals, rate swept (p50/p99 latency ms, forces/s)",
+        "config": {"workload": "force and leapfrog requests (1-100 steps, dt 1e-3), N log-uniform "
+                               "in [1024, 2^21], Plummer / Hernquist / uniform sphere, device "
+                               "resident", "requests": args.sweep_requests, "theta": THETA,
+                   "eps": EPS, "order": args.order, "mac": p.mac, "pipeline": p.pipeline,
+                   "lanes": args.lanes, "hbm_budget": 150e9,
+                   "median_n": int(np.median(sizes)), "max_n": int(max(sizes)),
+                   "force_evaluations": int(sum(sp[3] + 1 if sp[3] else 1 for sp in specs))},
+        "capacity": {"requests_per_s": cap_rps, "forces_per_s": cap["forces_per_s"],
+                     "p50_ms": cap["p50_ms"], "p99_ms": cap["p99_ms"]},
+        "rates": rates}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.serving_sweep:
+        run_serving_sweep(args)
     else:
         run_ours(args)
 
