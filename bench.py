@@ -99,6 +99,8 @@ def parse():
                     help="FP32 walk: 0 one warp per group, 1 producer/consumer warp teams "
                          "(the library default)")
     ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--tick-systems", type=int, default=2,
+                    help="served: systems of N bodies one lane's tick may hold")
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--split-system", action="store_true",
                     help="strong scaling: every rank takes the same system and walks its share of "
@@ -315,10 +317,13 @@ def run_ours(args):
             """Submits ``warm`` and waits, then submits all of ``reqs`` at
             once; returns (device ms from first submission to the last result,
             metrics of ``reqs``)."""
-            with serving.Server(p, device=local, lanes=args.lanes, max_tick_bodies=2 * n,
-                                hbm_budget=150e9) as srv:
-                for r in warm:
-                    srv.submit(r)
+            with serving.Server(p, device=local, lanes=args.lanes,
+                                max_tick_bodies=args.tick_systems * n, hbm_budget=150e9) as srv:
+                srv.submit_many(warm)
+                # the client allocates its requests' result buffers ahead of
+                # time (device requests) or pins them (host requests)
+                for r in reqs:
+                    srv.prepare(r)
                 srv.drain(timeout=600)
                 torch.cuda.synchronize()
                 if world > 1:
@@ -332,7 +337,7 @@ def run_ours(args):
                 t0 = time.perf_counter()
                 for r in reqs:
                     r.arrival = t0
-                    srv.submit(r)
+                srv.submit_many(reqs)
                 srv.drain(timeout=600)
                 torch.cuda.synchronize()
                 b.record(stream)
@@ -764,19 +769,21 @@ def run_serving_sweep(args):
     def run(reqs, rate=None):
         with serving.Server(p, device=local, lanes=args.lanes, hbm_budget=150e9) as srv:
             warm = sorted(requests(), key=lambda r: r.n * r.evals_needed)[:3]
-            for r in warm:                                # warm-up: the 3 smallest
-                srv.submit(r)
+            srv.submit_many(warm)                         # warm-up: the 3 smallest
+            for r in reqs:                                # result buffers, ahead of time
+                srv.prepare(r)
             srv.drain(timeout=1200)
-            t0 = time.perf_counter()
-            gaps = rng.exponential(1.0 / rate, len(reqs)) if rate else np.zeros(len(reqs))
-            t_next = t0
-            for r, g in zip(reqs, gaps):
-                t_next += g
-                delay = t_next - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                r.arrival = time.perf_counter()
-                srv.submit(r)
+            if rate is None:                              # all at once
+                srv.submit_many(reqs)
+            else:                                         # Poisson arrivals
+                t_next = time.perf_counter()
+                for r, g in zip(reqs, rng.exponential(1.0 / rate, len(reqs))):
+                    t_next += g
+                    delay = t_next - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    r.arrival = time.perf_counter()
+                    srv.submit(r)
             srv.drain(timeout=1200)
             torch.cuda.synchronize()
             return srv.metrics(reqs)

@@ -350,11 +350,14 @@ class Server:
         return RESIDENT_BYTES_PER_BODY * n
 
     # -- client side --
-    def submit(self, r: Request) -> Request:
+    def _check_fits(self, r: Request) -> None:
         if r.n > self.max_tick_bodies:
             raise ValueError(f"request of {r.n} bodies exceeds a lane's tick ({self.max_tick_bodies})")
         if self.footprint(r.n) > self.hbm_budget - self.workspace_bytes:
             raise ValueError("request larger than the HBM budget")
+
+    def submit(self, r: Request) -> Request:
+        self._check_fits(r)
         self.prepare(r)
         if r.arrival is None:
             r.arrival = time.perf_counter()
@@ -363,6 +366,29 @@ class Server:
             self._inflight += 1
             self._cv.notify_all()
         return r
+
+    def submit_many(self, requests) -> list[Request]:
+        """Submits requests that arrive together: all are checked and prepared
+        first, then queued at once, so the lanes see the whole group when they
+        wake.  (Submitting them one by one lets the lanes start ticks on the
+        first arrivals while the client, competing with them for the
+        interpreter lock, is still submitting the rest: fewer systems per tick
+        and idle gaps on the device.)  Arrival times not set are set to the
+        moment of queueing."""
+        rs = list(requests)
+        for r in rs:
+            self._check_fits(r)
+        for r in rs:
+            self.prepare(r)
+        now = time.perf_counter()
+        for r in rs:
+            if r.arrival is None:
+                r.arrival = now
+        with self._cv:
+            self._pending.extend(rs)
+            self._inflight += len(rs)
+            self._cv.notify_all()
+        return rs
 
     @staticmethod
     def prepare(r: Request) -> Request:

@@ -174,3 +174,23 @@ def test_device_requests_match_plain_path(sv, lanes):
             qe, pe = plain_leapfrog(e[1], e[2], e[3], e[4], 1e-3)
             assert np.array_equal(r.q_out.cpu().numpy(), qe)
             assert np.array_equal(r.p_out.cpu().numpy(), pe)
+
+
+def test_submit_many_queues_a_group_at_once(sv):
+    """Requests submitted together (submit_many) get the plain path's results
+    bit for bit; a group holding a request that cannot fit is refused before
+    any of it is queued."""
+    reqs = mixed_requests(sv, 8, seed=11)
+    with sv.Server(lanes=2, max_tick_bodies=1 << 16, hbm_budget=40e9, **PARAMS) as srv:
+        out = srv.submit_many(reqs)
+        assert out == reqs and all(r.arrival is not None for r in reqs)
+        srv.drain(timeout=300)
+    for r in reqs:
+        assert r.error is None
+        check_against_plain(r)
+    m, q, _ = ic(3000, 6)
+    small = sv.Request("force", *ic(500, 7)[:2])
+    srv = sv.Server(max_tick_bodies=1024, hbm_budget=1e9, **PARAMS)
+    with pytest.raises(ValueError):
+        srv.submit_many([small, sv.Request("force", m, q)])
+    assert len(srv._pending) == 0
