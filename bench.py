@@ -98,7 +98,7 @@ def parse():
     ap.add_argument("--pipeline", type=int, default=None,
                     help="FP32 walk: 0 one warp per group, 1 producer/consumer warp teams "
                          "(the library default)")
-    ap.add_argument("--lanes", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=3)
     ap.add_argument("--tick-systems", type=int, default=2,
                     help="served: systems of N bodies one lane's tick may hold")
     ap.add_argument("--batch-systems", type=int, default=512)
