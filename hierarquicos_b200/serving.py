@@ -115,8 +115,11 @@ class _Lane:
         cap, cap_s = server.max_tick_bodies, server.max_tick_systems
         with torch.cuda.device(dev):
             self.stream = torch.cuda.Stream(dev)
-            self.h2d = torch.cuda.Stream(dev)
-            self.d2h = torch.cuda.Stream(dev)
+            # host copies go through the server's two copy streams, shared by
+            # the lanes: in the order the lanes enqueue them, at the full
+            # bandwidth of each direction
+            self.h2d = server.h2d
+            self.d2h = server.d2h
             self.sys = BHSystem(dev.index).reserve(cap, cap_s)
             self.buf = [torch.empty(7, cap, dtype=torch.float64, device=dev) for _ in range(2)]
             self.out = torch.empty(3 * cap, dtype=torch.float64, device=dev)
@@ -340,6 +343,9 @@ class Server:
         self._inflight = 0
         self._lane_error = None
         self.completed: list[Request] = []
+        with torch.cuda.device(self.device):
+            self.h2d = torch.cuda.Stream(self.device)
+            self.d2h = torch.cuda.Stream(self.device)
         self.lanes = [_Lane(self, i) for i in range(lanes)]
         self._lane_bodies = [0] * lanes
         self._started = False
