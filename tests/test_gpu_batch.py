@@ -223,3 +223,40 @@ def test_batch_rejects_bad_layouts(bh):
     # and the handle still works afterwards
     f = s.forces_batch(m, *xyz(q), np.array([0, 50, 100]), theta=0.5)
     assert np.isfinite(f.cpu().numpy()).all()
+
+
+def test_capture_as_the_first_walk_of_a_process():
+    """A process whose first walk is recorded into a CUDA graph: the walk's
+    one-time launch set-up happens during the capture, and the replay still
+    equals a plain evaluation bit for bit (run in a fresh interpreter)."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = f"""
+import sys
+sys.path.insert(0, {root!r}); sys.path.insert(0, {os.path.join(root, 'tests')!r})
+import numpy as np, torch
+from conftest import plummer, xyz
+from hierarquicos_b200.system import BHSystem
+from hierarquicos_b200._lib import default_params
+for order in (4, 8):
+    m, q = plummer(5000, seed=4)
+    p = default_params(theta=0.5, eps=0.01, order=order)
+    dev = torch.device('cuda')
+    ins = [torch.as_tensor(np.ascontiguousarray(a), device=dev) for a in (m, *xyz(q))]
+    s = BHSystem()
+    s.build_batch(*ins, np.array([0, 5000]), p)
+    s.sync()
+    out = torch.zeros(15000, dtype=torch.float64, device=dev)
+    s.capture(p, out)
+    s.replay()
+    s.sync()
+    ref = BHSystem().forces(*ins, p)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref), order
+print('ok')
+"""
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
