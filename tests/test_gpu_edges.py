@@ -126,6 +126,12 @@ def test_invalid_arguments(api):
         api.compute_forces(m, *xyz(q), -1.0, 1.0, 0.0, True)
     with pytest.raises(api.BHError):
         api.compute_forces(m[:50], *xyz(q), 0.5, 1.0, 0.0, True)
+    from hierarquicos_b200.system import BHSystem
+
+    for bad in (dict(pipeline=2), dict(pipeline=-1), dict(mac=2)):
+        with pytest.raises(api.BHError) as e:
+            BHSystem().forces(m, *xyz(q), **bad)
+        assert e.value.code == 1, bad
 
 
 def test_theta_zero_is_direct(api):
