@@ -3,15 +3,17 @@
 
 Headline (default): force evaluations of N = 1,048,576-body Hernquist systems
 (a = 1, truncated at 100 a, equal masses, seeded; theta = 0.5, quadrupole,
-softening 0.01, FP32 Kahan-compensated group walk), served by the continuous
+softening 0.01, FP32 Kahan-compensated group walk: producer/consumer warp
+teams, box test plus every member's own MAC), served by the continuous
 batching server against the plain single-system call:
 
   * plain  -- ``bh_system_forces`` per system (keys -> radix sort -> octree ->
     multipoles -> groups -> walk -> status), device-resident inputs, the L2
     flushed before every call;
   * served -- the same systems submitted at once to ``serving.Server``
-    (2 lanes, continuous batching), device-resident requests; p50/p99 latency
-    per request;
+    (3 lanes, ticks of up to 2 systems, continuous batching), device-resident
+    requests prepared ahead (result buffers allocated) and queued together
+    with ``submit_many``; p50/p99 latency per request;
   * e2e    -- both again from pinned HOST buffers with the copies included:
     plain through ``bh_compute_forces_ex`` (the api3d drop-in), served with
     host requests;
@@ -27,6 +29,7 @@ seeded targets; served results are checked equal (bit for bit) to the plain
 ones.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --serving-sweep     # the serving config: Poisson arrivals, rate swept
 
 One process per GPU (torchrun for N > 1): every rank serves its own systems
 (weak scaling, no collective on the data path); times are the max over
