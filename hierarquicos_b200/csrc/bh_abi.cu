@@ -505,6 +505,7 @@ void bh_params_default(bh_params *p) {
   p->leaf_cap = 8;
   p->com_mode = 1;
   p->strict_keys = 1;
+  p->mac = 1;
   p->pipeline = 1;
 }
 

@@ -76,7 +76,7 @@ typedef struct bh_params {
 
 /* Defaults: theta 0.5, G 1, eps 0, order 4, forces, depth 21, FP32, amp 1.2,
  * group 64, leaf_cap 8, com_mode 1, strict_keys 1, count_stats 0, group_span 0,
- * mac 0, pipeline 1. */
+ * mac 1, pipeline 1. */
 void bh_params_default(bh_params *p);
 
 const char *bh_version(void);
