@@ -36,7 +36,8 @@
 namespace {
 
 constexpr int64_t kMaxN = BH_NOALLOC_MAX_N;
-constexpr int64_t kSlots = 512;       // stacks of the walk (512 persistent one-warp blocks)
+constexpr int64_t kSlots = 512;       // walk stacks: 512 one-warp blocks, or 128 blocks of 4
+                                      // producer warps in the pipelined walk
 constexpr int64_t kStackCap = 1024;   // stack entries per warp slot
 constexpr int64_t kItems = (kMaxN + bh::kRedChunk - 1) / bh::kRedChunk;  // reduction items
 constexpr int kNumBufs = 36;
