@@ -39,7 +39,7 @@ EXPORTED = [
     "bh_system_reference_targets", "bh_probe_fma_peak", "bh_probe_bounded_wait", "bh_compute_forces_noalloc",
     "bh_system_build_batch", "bh_system_forces_batch", "bh_system_batch_info",
     "bh_system_capture", "bh_system_replay", "bh_kick_drift", "bh_diagnostics",
-    "bh_kick_drift_systems", "bh_generate_ics", "bh_system_reserve",
+    "bh_kick_drift_systems", "bh_generate_ics", "bh_system_reserve", "bh_system_get_key_checks",
 ]
 
 BH_NOALLOC_MAX_N = 8192
@@ -106,6 +106,7 @@ def lib():
             "bh_system_get_nodes": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
             "bh_system_get_groups": [_vp, _vp],
             "bh_system_get_stats": [_vp, _vp],
+            "bh_system_get_key_checks": [_vp, _vp],
             "bh_system_reference_targets": [_vp, C.POINTER(BHParams), _vp, _i64, _vp, _vp, _vp],
             "bh_probe_fma_peak": [_i, _vp],
             "bh_probe_bounded_wait": [_i, C.c_longlong, _vp],

@@ -9,6 +9,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -39,14 +40,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
+    cmds = []
     objs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc, *NVCC_FLAGS, "-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc, *NVCC_FLAGS, "-c", src, "-o", obj])
         objs.append(obj)
+    # one nvcc per source file, in parallel
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = LIB + ".tmp"
     # the CUDA runtime is linked statically (nvcc's default): the library does
     # not depend on which libcudart a host process has already loaded

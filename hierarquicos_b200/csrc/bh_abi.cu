@@ -22,6 +22,9 @@ struct bh_system {
   std::vector<bh::RedItem> items_host;
   int built = 0;
   int keys_checked = 0;   // strict-key check done for the current build
+  // strict-key slow path since creation: sequential centre-of-mass checks run,
+  // and builds redone because a key differed
+  int64_t key_checks = 0, key_rebuilds = 0;
   int order = 4;
   int64_t stack_cap = 4096;
   int fixed_buffers = 0;  // buffers provided by the caller: never reallocated
@@ -408,7 +411,9 @@ int finish(bh_system *s, cudaStream_t st) {
     bh::launch_verify_keys(s->x, s->y, s->z, s->n, all, s->b, st);
     rc = read_scalars(s, st);
     if (rc) return rc;
+    ++s->key_checks;
     if (s->b.sc_host->key_mismatch) {
+      ++s->key_rebuilds;
       bh::launch_adopt_seq_com(s->b, st);
       enqueue_build(s, 1, st);
       if (s->walked) {
@@ -768,6 +773,13 @@ int bh_system_get_stats(bh_system *s, uint64_t *stats4) {
   BH_CUDA(cudaSetDevice(s->device));
   BH_CUDA(cudaDeviceSynchronize());
   BH_CUDA(cudaMemcpy(stats4, s->b.stats, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  return BH_OK;
+}
+
+int bh_system_get_key_checks(bh_system *s, int64_t *checks2) {
+  if (!s || !checks2) return set_err(BH_ERR_INVALID, "NULL argument");
+  checks2[0] = s->key_checks;
+  checks2[1] = s->key_rebuilds;
   return BH_OK;
 }
 

@@ -12,7 +12,7 @@
 // Limits and behaviour:
 //  * at most BH_NOALLOC_MAX_N bodies (8192); larger n is rejected with
 //    BH_ERR_INVALID and a message;
-//  * the array (about 5.8 MB) lives on every device on which this library's
+//  * the array (about 7.9 MB) lives on every device on which this library's
 //    module holding it is loaded, until the process exits;
 //  * the first call on a device looks the array's device address up
 //    (cudaGetSymbolAddress, with that device current) and keeps it; later
@@ -23,9 +23,11 @@
 //    the GPU (other streams, other host threads) race on that array: issue
 //    them one after another.  Host threads are serialised by a lock, but work
 //    already queued on the GPU is not.
-//  * the walk stack is fixed (1024 entries per warp); a walk that would need
-//    more returns BH_ERR_CAPACITY instead of growing it.
-// The results are those of bh_system_forces on the same inputs and parameters.
+//  * the walk stacks are fixed, with room for every node of the largest tree
+//    (kMaxN entries per walking warp), so a walk never runs out of stack at
+//    any theta; the stacks are about 4 MB of the array.
+// The results are those of bh_system_forces on the same inputs and
+// parameters, bit for bit: the same kernels run in the same order.
 #include <stdio.h>
 
 #include <mutex>
@@ -36,9 +38,12 @@
 namespace {
 
 constexpr int64_t kMaxN = BH_NOALLOC_MAX_N;
-constexpr int64_t kSlots = 512;       // walk stacks: 512 one-warp blocks, or 128 blocks of 4
-                                      // producer warps in the pipelined walk
-constexpr int64_t kStackCap = 1024;   // stack entries per warp slot
+constexpr int64_t kSlots = 128;       // walk stacks: at most 128 walking warps (128 one-warp
+                                      // blocks, or 32 blocks of 4 producer warps), as many as
+                                      // there are 64-body groups in kMaxN bodies
+constexpr int64_t kStackCap = kMaxN;  // stack entries per warp: a group's walk pushes every
+                                      // node at most once and a tree of n bodies has fewer
+                                      // than n nodes, so the stack cannot overflow
 constexpr int64_t kItems = (kMaxN + bh::kRedChunk - 1) / bh::kRedChunk;  // reduction items
 constexpr int kNumBufs = 36;
 

@@ -1453,15 +1453,19 @@ template <typename T, int ORDER, int MAXTPL, bool SOFT>
 static void launch_group_walk(const WalkArgs &a, cudaStream_t s) {
   if (sizeof(T) == 4 && a.pipeline && launch_pipe_walk<ORDER, MAXTPL, SOFT>(a, s)) return;
   // exactly the blocks that are resident at once: no block waits for a
-  // second wave behind the walk (which would also hold back other streams)
-  static int per_sm = 0;
-  if (per_sm == 0) {
+  // second wave behind the walk (which would also hold back other streams);
+  // occupancy is a property of the device, so it is kept per device
+  static int per_sm[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (per_sm[dev] == 0) {
     int v = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, group_walk_kernel<T, ORDER, MAXTPL, SOFT>,
                                                   kWarp, 0);
-    per_sm = v > 0 ? v : 1;
+    per_sm[dev] = v > 0 ? v : 1;
   }
-  int64_t blocks = (int64_t)per_sm * sm_count();
+  int64_t blocks = (int64_t)per_sm[dev] * sm_count();
   if (blocks > a.slots) blocks = a.slots;
   group_walk_kernel<T, ORDER, MAXTPL, SOFT><<<(unsigned)blocks, kWarp, 0, s>>>(a);
 }

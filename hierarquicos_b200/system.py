@@ -198,6 +198,13 @@ class BHSystem:
         check(lib().bh_system_get_groups(self._h, g.ctypes.data_as(C.c_void_p)))
         return g
 
+    def key_checks(self) -> tuple[int, int]:
+        """(sequential centre-of-mass checks, rebuilds) of the strict-key path
+        since this handle was created."""
+        c = np.zeros(2, np.int64)
+        check(lib().bh_system_get_key_checks(self._h, c.ctypes.data_as(C.c_void_p)))
+        return int(c[0]), int(c[1])
+
     def stats(self) -> np.ndarray:
         s = np.zeros(4, np.uint64)
         check(lib().bh_system_get_stats(self._h, s.ctypes.data_as(C.c_void_p)))

@@ -203,6 +203,14 @@ int bh_system_get_groups(bh_system *sys, int32_t *group_first);
  * in bh_params): [0] body-body, [1] body-cell, [2] groups, [3] node tests. */
 int bh_system_get_stats(bh_system *sys, uint64_t *stats4);
 
+/* Strict-key slow path of this handle since its creation (strict_keys 1/2 in
+ * bh_params): checks2[0] = completed builds for which the reference's
+ * sequential centre of mass (morton_octree.f90:364-370) was computed because
+ * a body lay within the rounding margin of a cell edge (or strict_keys 2);
+ * checks2[1] = builds redone because a key differed.  Host counters: no
+ * device work, no synchronisation. */
+int bh_system_get_key_checks(bh_system *sys, int64_t *checks2);
+
 /* Per-target FP64 walk with the reference's semantics on a subset of targets
  * (DEVICE arrays, original indices); counts (optional, device, 2 per target):
  * body-body and cell interactions. */
@@ -214,7 +222,7 @@ int bh_system_reference_targets(bh_system *sys, const bh_params *p, const int64_
  * memory (their memory belongs to another allocator, a cudaMalloc would stall
  * their time-step loop, or their host forbids it).  No counterpart in the
  * reference.  Device inputs and output as bh_system_forces; everything else
- * comes from one fixed device array of about 5.8 MB inside the library, so n
+ * comes from one fixed device array of about 7.9 MB inside the library, so n
  * is limited to BH_NOALLOC_MAX_N (larger n: BH_ERR_INVALID).  The first call on
  * a device looks that array up; all calls on a device share it, so calls that
  * overlap on the GPU race: run them one after another.  Synchronous. */

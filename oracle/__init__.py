@@ -38,10 +38,48 @@ def build(force: bool = False) -> str:
     return _SO
 
 
+def _host_tag() -> str:
+    """The CPU model and flags of this host, hashed: a -march=native build is
+    only valid on a host with the same tag."""
+    import hashlib
+    import platform
+
+    info = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
+
+
+def use_native_build() -> str:
+    """Switches this process to the timed CPU-baseline build of the same
+    source (the reference's flags: -O3 -march=native -fopenmp, contraction
+    allowed), compiled for this host on first use.  Call before anything
+    else in the process uses the oracle; the parity checks use the default
+    build."""
+    global _SO
+    if _lib is not None:
+        raise RuntimeError("use_native_build() must come before the oracle is first loaded")
+    rel = os.path.join("_build", f"native-{_host_tag()}")
+    so = os.path.join(_HERE, rel, "libbh_oracle.so")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(
+            os.path.join(_HERE, "bh_oracle.c")):
+        subprocess.run(["make", "-s", "-C", _HERE, "fast", f"FASTDIR={rel}"], check=True)
+    _SO = so
+    return so
+
+
 def lib():
     global _lib
     if _lib is None:
-        build()
+        if _SO.endswith(os.path.join("_build", "libbh_oracle.so")):
+            build()
         L = C.CDLL(_SO)
         L.orc_last_error.restype = C.c_char_p
         L.orc_argsort.argtypes = [C.c_int64, _u64p, _i32p]
@@ -57,6 +95,7 @@ def lib():
         L.orc_morton_get_nodes.argtypes = [C.c_void_p] + [C.c_void_p] * 12
         L.orc_morton_forces.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
                                         _dp, C.c_int]
+        L.orc_morton_octupoles.argtypes = [C.c_void_p]
         L.orc_morton_forces_targets.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                                 C.c_int, C.c_int64, _i64p, _dp, C.c_void_p, C.c_int]
         L.orc_morton_dehnen.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -172,12 +211,21 @@ class MortonTree:
         lib().orc_morton_get_nodes(self._h, *[_ptr(d[k]) for k in order])
         return d
 
-    def forces_par(self, G: float, eps2: float, theta2: float, mult: bool | None = None,
+    def _mult(self, mult) -> int:
+        """True/False (the reference's quadrupole switch) or 8: the octupole
+        terms of octree_default.f90:1012-1063 over this tree."""
+        if mult is None or mult is True:
+            return 1
+        if mult == 8:
+            _check(lib().orc_morton_octupoles(self._h))
+            return 8
+        return int(bool(mult))
+
+    def forces_par(self, G: float, eps2: float, theta2: float, mult: bool | int | None = None,
                    nthreads: int = 0) -> np.ndarray:
         """Forces (N,3) in original order; memory layout SoA like api3d."""
         out = np.empty(3 * self.n)
-        mult = True if mult is None else mult
-        _check(lib().orc_morton_forces(self._h, G, eps2, theta2, int(mult), out, nthreads))
+        _check(lib().orc_morton_forces(self._h, G, eps2, theta2, self._mult(mult), out, nthreads))
         return out.reshape(3, self.n).T
 
     def dehnen(self, G: float, eps2: float, theta2: float, mult: int = 4, pairs: bool = False):
@@ -195,8 +243,8 @@ class MortonTree:
         t = np.ascontiguousarray(targets, dtype=np.int64)
         out = np.empty(3 * t.size)
         cnt = np.empty(2 * t.size, np.int64)
-        _check(lib().orc_morton_forces_targets(self._h, G, eps2, theta2, int(mult), t.size, t, out,
-                                               _ptr(cnt), nthreads))
+        _check(lib().orc_morton_forces_targets(self._h, G, eps2, theta2, self._mult(mult), t.size,
+                                               t, out, _ptr(cnt), nthreads))
         return out.reshape(3, t.size).T, cnt.reshape(t.size, 2)
 
 

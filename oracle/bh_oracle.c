@@ -18,7 +18,7 @@
  * Fortran compiler), and its own tests store no expected keys, permutations,
  * topologies or forces.  This restatement is therefore pinned only
  * statistically, against the force-error statistics the reference recorded in
- * benchmarks/forces_time_and_error/out/ (see tests/test_oracle_pin.py).
+ * benchmarks/forces_time_and_error/out/ (see tests/test_oracle.py).
  *
  * Floating point: compile with -ffp-contract=off.  Each Fortran operation is
  * then rounded separately, which is the semantics of the source text.  The one
@@ -220,6 +220,7 @@ typedef struct {
     int64_t *prefix;
     int32_t *level, *first, *last, *parent, *nchild, *child, *next;
     double *size2, *nmass, *qcm, *quad;
+    double *oct;        /* 14 per node, only after orc_morton_octupoles */
 } orc_morton;
 
 void orc_morton_free(orc_morton *t) {
@@ -228,7 +229,7 @@ void orc_morton_free(orc_morton *t) {
     free(t->level_begin); free(t->level_end);
     free(t->prefix); free(t->level); free(t->first); free(t->last); free(t->parent);
     free(t->nchild); free(t->child); free(t->next);
-    free(t->size2); free(t->nmass); free(t->qcm); free(t->quad);
+    free(t->size2); free(t->nmass); free(t->qcm); free(t->quad); free(t->oct);
     free(t);
 }
 
@@ -454,10 +455,40 @@ int orc_morton_get_nodes(const orc_morton *t, int64_t *prefix, int32_t *level, d
     return ORC_OK;
 }
 
+/* The octupole part of a cell's field, octree_default.f90:1012-1063 (the
+ * insertion tree's bh_forces_over_p), on the raw third moments o[14] of the
+ * node about its centre of mass: the same expression as octree_walk below.
+ * invR, invR2 and invR5 are of the softened distance. */
+static void octupole_terms(const double *o, double dx, double dy, double dz, double invR,
+                           double invR2, double invR5, double O[3]) {
+    (void)invR2;
+    double invR7 = invR5 * invR * invR;
+    double invR9 = invR7 * invR * invR;
+    double Ox = -1.5 * invR5 * o[11];
+    double Oy = -1.5 * invR5 * o[12];
+    double Oz = -1.5 * invR5 * o[13];
+    double Oc = 7.5 * invR7 * (dx * o[11] + dy * o[12] + dz * o[13]);
+    Ox = Ox + dx * Oc; Oy = Oy + dy * Oc; Oz = Oz + dz * Oc;
+    double ddx = dx * dx, ddy = dy * dy, ddz = dz * dz;
+    Ox = Ox + 7.5 * invR7 * (ddx * o[0] + ddy * o[1] + ddz * o[2] + 2.0 * dx * dy * o[3] +
+                             2.0 * dx * dz * o[6] + 2.0 * dy * dz * o[9]);
+    Oy = Oy + 7.5 * invR7 * (ddx * o[3] + ddy * o[4] + ddz * o[5] + 2.0 * dx * dy * o[1] +
+                             2.0 * dx * dz * o[9] + 2.0 * dy * dz * o[7]);
+    Oz = Oz + 7.5 * invR7 * (ddx * o[6] + ddy * o[7] + ddz * o[8] + 2.0 * dx * dy * o[9] +
+                             2.0 * dx * dz * o[2] + 2.0 * dy * dz * o[5]);
+    Oc = -17.5 * invR9 *
+         (ddx * dx * o[0] + ddy * dy * o[4] + ddz * dz * o[8] + 3.0 * ddx * dy * o[3] +
+          3.0 * ddx * dz * o[6] + 3.0 * ddy * dx * o[1] + 3.0 * ddy * dz * o[7] +
+          3.0 * ddz * dx * o[2] + 3.0 * ddz * dy * o[5] + 6.0 * dx * dy * dz * o[9]);
+    O[0] = Ox + dx * Oc; O[1] = Oy + dy * Oc; O[2] = Oz + dz * Oc;
+}
+
 /* morton_octree.f90:627-766 (barnes_hut): stackless walk over `next` links for
  * sorted particle p.  Returns the force (G m_p a_p).  cnt[0] counts body-body
  * interactions (leaf particles and single-particle nodes), cnt[1] counts
- * multipole (quadrupole) cell interactions. */
+ * multipole (quadrupole) cell interactions.  mult 0 monopole, 1 quadrupole
+ * (the reference's two options); mult 8 adds the octupole terms of the
+ * insertion tree's walk to the quadrupole (needs orc_morton_octupoles). */
 static void morton_walk(const orc_morton *t, int64_t p, double theta2, double G, double eps2,
                         int mult, double f[3], int64_t cnt[2]) {
     double mp = t->ms[p];
@@ -520,9 +551,11 @@ static void morton_walk(const orc_morton *t, int64_t p, double theta2, double G,
                     Qx = Qx + mxyi * dy * dx2 + mxzi * dz * dx2 + myzi * dxyz;
                     Qy = Qy + myzi * dz * dy2 + mxyi * dx * dy2 + mxzi * dxyz;
                     Qz = Qz + mxzi * dx * dz2 + myzi * dy * dz2 + mxyi * dxyz;
-                    fx = fx + G * mp * (mx + invR5 * Qx);
-                    fy = fy + G * mp * (my + invR5 * Qy);
-                    fz = fz + G * mp * (mz + invR5 * Qz);
+                    double O[3] = {0.0, 0.0, 0.0};
+                    if (mult == 8) octupole_terms(t->oct + 14 * idx, dx, dy, dz, invR, invR2, invR5, O);
+                    fx = fx + G * mp * (mx + invR5 * Qx + O[0]);
+                    fy = fy + G * mp * (my + invR5 * Qy + O[1]);
+                    fz = fz + G * mp * (mz + invR5 * Qz + O[2]);
                     npc++;
                 }
             }
@@ -535,12 +568,36 @@ static void morton_walk(const orc_morton *t, int64_t p, double theta2, double G,
     if (cnt) { cnt[0] = npp; cnt[1] = npc; }
 }
 
+static void direct_moments(const orc_morton *t, int64_t first, int64_t last, const double c[3],
+                           double *Q, double *O);
+
+/* Raw third moments of every node about its centre of mass, summed directly
+ * over the node's particles with the summary sums of octree_default.f90
+ * :875-880 (the Morton module itself stops at the quadrupole).  Lets the walk
+ * above run with mult 8: the Morton tree's topology with the octupole terms
+ * of octree_default.f90:1012-1063. */
+int orc_morton_octupoles(orc_morton *t) {
+    if (t->oct) return ORC_OK;
+    t->oct = (double *)malloc((size_t)t->nnodes * 14 * sizeof(double));
+    if (!t->oct) return fail(ORC_ENOMEM, "octupoles: out of memory");
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 256)
+#endif
+    for (int64_t j = 0; j < t->nnodes; ++j) {
+        double Q[6];
+        if (t->first[j] < 0) { for (int k = 0; k < 14; ++k) t->oct[14 * j + k] = 0.0; continue; }
+        direct_moments(t, t->first[j], t->last[j], t->qcm + 3 * j, Q, t->oct + 14 * j);
+    }
+    return ORC_OK;
+}
+
 /* morton_octree.f90:150-180 (forces_par): forces for every particle, written
  * back through the permutation into ORIGINAL order.  out is SoA: fx[n], fy[n],
  * fz[n] (the memory layout of the api3d (N,3) Fortran result). */
 int orc_morton_forces(const orc_morton *t, double G, double eps2, double theta2, int mult,
                       double *out, int nthreads) {
     int64_t n = t->n;
+    if (mult == 8 && !t->oct) return fail(ORC_EINVAL, "forces: mult 8 needs orc_morton_octupoles");
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
@@ -561,6 +618,7 @@ int orc_morton_forces_targets(const orc_morton *t, double G, double eps2, double
                               int64_t nt, const int64_t *targets, double *out, int64_t *counts,
                               int nthreads) {
     int64_t n = t->n;
+    if (mult == 8 && !t->oct) return fail(ORC_EINVAL, "targets: mult 8 needs orc_morton_octupoles");
     int32_t *inv = (int32_t *)malloc((size_t)n * sizeof(int32_t));
     if (!inv) return fail(ORC_ENOMEM, "targets: out of memory");
     for (int64_t p = 0; p < n; ++p) inv[t->perm[p]] = (int32_t)p;

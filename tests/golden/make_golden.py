@@ -9,14 +9,15 @@
    dehnen_{monopole,quadrupole}.txt (benchmarks/dehnen/forces_dehnen.f90:
    13-153, the same spheres, N = 5000 and 10000, 6 draws, methods 20/21).
    For each (order, N, theta) the median and the 10th/90th percentiles of the
-   recorded normalised RMS error are stored.  Needs the reference checkout
-   (REFERENCE_ROOT, default /root/reference); run only where it exists.
+   recorded normalised RMS error are stored.  Needs a checkout of the
+   reference, named by the REFERENCE_ROOT environment variable; without it
+   this part is skipped.
 
 2. oracle_small.npz -- keys, permutation and forces of the CPU oracle on small
    seeded inputs, so that a change to the oracle is caught even without the
    reference.
 
-Usage: python tests/golden/make_golden.py
+Usage: REFERENCE_ROOT=<checkout of the reference> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -31,7 +32,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
-REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT")
 
 
 def recorded_errors():
@@ -97,6 +98,8 @@ def oracle_small():
 
 
 if __name__ == "__main__":
-    if os.path.isdir(REFERENCE_ROOT):
+    if REFERENCE_ROOT and os.path.isdir(REFERENCE_ROOT):
         recorded_errors()
+    else:
+        print("REFERENCE_ROOT not set: recorded_errors.json left as it is")
     oracle_small()

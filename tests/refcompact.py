@@ -8,30 +8,36 @@ import numpy as np
 
 
 def compact_from_reference(nodes: dict):
+    """(ref_ids, meta (M,4), children (M,8), nchildren (M,)) of the compact
+    tree.  meta = first, count, level, nchild.  A child is the compact index of
+    the deepest link of its chain, or ~first for a lone particle; entries at or
+    beyond nchildren are 0.  Vectorised over the levels (nodes are stored level
+    by level, children after parents), so it runs on 10^7-node trees."""
     level, first, last = nodes["level"], nodes["first"], nodes["last"]
     nchild, child = nodes["nchild"], nodes["child"]
-    is_compact = (last > first) & (nchild != 1)
+    nn = level.size
+    multi = last > first
+    is_compact = multi & (nchild != 1)
     ref_ids = np.nonzero(is_compact)[0]            # already in (level, first) order
-    cidx = -np.ones(level.size, np.int64)
+    cidx = np.full(nn, -1, np.int64)
     cidx[ref_ids] = np.arange(ref_ids.size)
-
-    def deepest(r):
-        while nchild[r] == 1 and last[r] > first[r]:
-            r = child[r, 0]
-        return r
-
-    meta = np.stack([first[ref_ids], last[ref_ids] - first[ref_ids] + 1, level[ref_ids],
-                     np.where(nchild[ref_ids] == 0, 0, nchild[ref_ids])], axis=1).astype(np.int64)
-    children = []
-    for r in ref_ids:
-        ch = []
-        for c in child[r, : nchild[r]]:
-            if last[c] > first[c]:
-                ch.append(int(cidx[deepest(c)]))
-            else:
-                ch.append(int(~first[c]))
-        children.append(ch)
-    return ref_ids, meta, children
+    # deepest link of every chain, from the deepest level up
+    deep = np.arange(nn, dtype=np.int64)
+    chain = multi & (nchild == 1)
+    top = int(level.max()) if nn else 0
+    bounds = np.searchsorted(level, np.arange(top + 2), side="left")
+    for lv in range(top, -1, -1):
+        a, b = bounds[lv], bounds[lv + 1]
+        r = a + np.nonzero(chain[a:b])[0]
+        deep[r] = deep[child[r, 0]]
+    nch = np.where(nchild[ref_ids] == 0, 0, nchild[ref_ids]).astype(np.int64)
+    meta = np.stack([first[ref_ids], last[ref_ids] - first[ref_ids] + 1, level[ref_ids], nch],
+                    axis=1).astype(np.int64)
+    used = np.arange(8)[None, :] < nch[:, None]
+    ch = np.where(used, child[ref_ids], 0)
+    val = np.where(multi[ch], cidx[deep[ch]], ~first[ch].astype(np.int64))
+    children = np.where(used, val, 0)
+    return ref_ids, meta, children, nch
 
 
 def exact_octupole(spos_m, spos_x, meta, com):
