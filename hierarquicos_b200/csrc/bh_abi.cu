@@ -25,6 +25,7 @@ struct bh_system {
   // strict-key slow path since creation: sequential centre-of-mass checks run,
   // and builds redone because a key differed
   int64_t key_checks = 0, key_rebuilds = 0;
+  int64_t walks_enqueued = 0;  // every walk put on a stream (a redone walk included)
   int order = 4;
   int64_t stack_cap = 4096;
   int fixed_buffers = 0;  // buffers provided by the caller: never reallocated
@@ -337,6 +338,7 @@ bh::WalkParams walk_params(const bh_params *p, int order) {
 
 // the walk of the whole batch, enqueued without host synchronisation
 int enqueue_walk(bh_system *s, const bh_params *p, double *d_out, cudaStream_t st) {
+  ++s->walks_enqueued;
   bh::WalkParams w = walk_params(p, s->order);
   w.g_begin = s->walk_g0;
   w.g_end = s->walk_g1;
@@ -812,9 +814,19 @@ int bh_compute_forces_ex(const double *m, const double *x, const double *y, cons
   rc = stage_inputs(s, m, x, y, z, n, st);
   if (rc) return rc;
   Buffers &b = s->b;
-  rc = bh_system_forces(s, b.hm, b.hx, b.hy, b.hz, n, p, b.hout, stream);
+  rc = bh_system_build(s, b.hm, b.hx, b.hy, b.hz, n, p, stream);
   if (rc) return rc;
+  rc = bh_system_walk(s, p, b.hout, stream);
+  if (rc) return rc;
+  // the result's copy goes on the stream before the status is read, so it
+  // follows the walk without a host round trip; if the status check redoes
+  // the walk (strict-key rebuild, larger stack) the copy is made again
+  const int64_t walks = s->walks_enqueued;
   BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  rc = finish(s, st);
+  if (rc) return rc;
+  if (s->walks_enqueued != walks)
+    BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
   BH_CUDA(cudaStreamSynchronize(st));
   return BH_OK;
 }

@@ -7,7 +7,7 @@
 // extent (rmax 0), a node's children are its child nodes and lone bodies, or,
 // for a node of identical keys, its bodies.
 //
-//  1. rmax (evaluate_rmax :1095-1131), level by level from the deepest: the
+//  1. rmax (evaluate_rmax :1095-1131), from the leaves up in one launch: the
 //     largest distance from a node's centre of mass to any child's centre of
 //     mass plus that child's rmax (massless children skipped).
 //  2. Dual traversal (mutual_interaction_walk_* :1133-1402) as a sequence of
@@ -16,13 +16,18 @@
 //     a's children (i <= j; a body with itself is dropped); a pair with
 //     (rmax_a + rmax_b)^2 <= theta^2 |z_a - z_b|^2 is a mutual interaction;
 //     otherwise the member with the larger rmax (a on ties) is replaced by its
-//     children.  Each generation is one launch over the previous one's pairs;
-//     the lists live in preallocated buffers whose fill the host reads once at
-//     the end, growing them and repeating when one overflowed.
+//     children.  Each generation is one launch over the previous one's pairs,
+//     a deterministic compaction (a chained scan over tiles of input pairs):
+//     the new frontier and the mutual pairs come out in input order, so both
+//     lists have one order whatever the schedule, and a system's pairs keep
+//     their relative order inside a batch.  The lists live in preallocated
+//     buffers whose fill the host reads once at the end, growing them and
+//     repeating when one overflowed.
 //  3. Each mutual pair (a, b) becomes the two one-sided terms (a <- b) and
-//     (b <- a) of :1200-1221, keyed (target, source) and radix-sorted, so every
-//     target sums its terms in one fixed order (results do not depend on the
-//     schedule nor on the other systems of a batch).  Term (t <- s), with
+//     (b <- a) of :1200-1221, keyed by target and sorted stably (radix passes
+//     over the target id only), so every target sums its terms in the mutual
+//     list's fixed order (results do not depend on the schedule nor on the
+//     other systems of a batch).  Term (t <- s), with
 //     R = z_t - z_s (evaluate_mutual_interaction_* :1425-1558):
 //       field  += M_s (D1 + Q_s : D3 / (2 M_s))      D1 = -G R r^-3
 //       hess   += M_s D2,  third += M_s D3           (r^2 = R^2 + eps^2)
@@ -30,10 +35,12 @@
 //                 C_jkl = M_s O_t,jkl - M_t O_s,jkl, c_j = C_jkk
 //     which is the reference's update of both nodes written once per side.
 //     Terms between coincident points without softening (r = 0) are skipped.
-//  4. Downward pass (dehnen_forces :1560-1673), level by level from the root:
-//     child field += parent field + H d + d.T.d / 2, child hessian += H + T d,
-//     child third += T, d = child centre of mass - parent's.  A body's force is
-//     m times its field.
+//  4. Downward pass (dehnen_forces :1560-1673): child field += parent field +
+//     H d + d.T.d / 2, child hessian += H + T d, child third += T, d = child
+//     centre of mass - parent's.  The translation of this cubic expansion is
+//     exact, so one launch lets every body sum its ancestors' own expansions
+//     translated straight to it (down_bodies_kernel) instead of pushing level
+//     by level.  A body's force is m times its field.
 #include "bh_internal.cuh"
 
 namespace bh {
@@ -68,84 +75,184 @@ __device__ __forceinline__ int64_t node_child(const Ent &e, int64_t j, int4 mt, 
   return e.n + mt.x + k;
 }
 
-__global__ void __launch_bounds__(128)
-rmax_level_kernel(int level, const int32_t *__restrict__ level_begin, Ent e, double *rmax) {
-  const int lb = level_begin[level], le = level_begin[level + 1];
-  for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x) {
-    const int4 mt = e.meta[j];
-    const double4 c = e.com[j];
-    double r = 0.0;
-    const int k = node_nchild(mt);
-    for (int q = 0; q < k; ++q) {
-      const int64_t ch = node_child(e, j, mt, q);
-      const double4 cc = ent_com(e, ch);
-      if (cc.w == 0.0) continue;
-      const double dx = cc.x - c.x, dy = cc.y - c.y, dz = cc.z - c.z;
-      const double v = sqrt(dx * dx + dy * dy + dz * dz) + ent_rmax(e, ch);
-      if (v > r) r = v;
+// rmax of node j from its children (evaluate_rmax, octree_default.f90:1095-1131);
+// the children's rmax is read through L2 (ld.cg) because another thread of
+// the same launch may have written it.
+__device__ __forceinline__ double node_rmax(const Ent &e, int j) {
+  const int4 mt = e.meta[j];
+  const double4 c = e.com[j];
+  double r = 0.0;
+  const int k = node_nchild(mt);
+  for (int q = 0; q < k; ++q) {
+    const int64_t ch = node_child(e, j, mt, q);
+    const double4 cc = ent_com(e, ch);
+    if (cc.w == 0.0) continue;
+    const double dx = cc.x - c.x, dy = cc.y - c.y, dz = cc.z - c.z;
+    const double v = sqrt(dx * dx + dy * dy + dz * dz) + (ch < e.n ? __ldcg(e.rmax + ch) : 0.0);
+    if (v > r) r = v;
+  }
+  return r;
+}
+
+__device__ __forceinline__ int node_children_count(const Ent &e, int j) {
+  const int4 mt = e.meta[j];
+  if (mt.w == 0) return 0;
+  int k = 0;
+  for (int q = 0; q < mt.w; ++q) k += e.child[8 * (int64_t)j + q] >= 0 ? 1 : 0;
+  return k;
+}
+
+// All of evaluate_rmax in one launch, bottom-up with an arrival counter per
+// node (the scheme of the upward pass): a thread starts at every node without
+// node children, and the last child to arrive at a parent goes on with it.
+// Every node is computed once, after its children, with the same arithmetic
+// as the level-by-level form.  A chain longer than the deepest tree raises
+// kErrIndex instead of looping.
+__global__ void __launch_bounds__(256)
+rmax_fused_kernel(const Scalars *__restrict__ scr, Ent e, const int32_t *__restrict__ parent,
+                  double *rmax, int32_t *arrive, int *err) {
+  const int M = scr->n_compact;
+  for (int j0 = blockIdx.x * blockDim.x + threadIdx.x; j0 < M; j0 += gridDim.x * blockDim.x) {
+    if (node_children_count(e, j0) != 0) continue;
+    int j = j0;
+    for (int step = 0;; ++step) {
+      if (step > kNumLevels + 1) { atomicOr(err, kErrIndex); break; }
+      rmax[j] = node_rmax(e, j);
+      const int p = parent[j];
+      if (p < 0) break;
+      const int need = node_children_count(e, p);
+      __threadfence();
+      if (atomicAdd(&arrive[p], 1) != need - 1) break;
+      __threadfence();
+      j = p;
     }
-    rmax[j] = r;
   }
 }
 
+// The first frontier: (root, root) of every system, in system order (a
+// system without a tree contributes (-1, -1), which the traversal drops).
 __global__ void roots_frontier_kernel(const SysScalars *__restrict__ ss, int nsys, int2 *fout,
                                       unsigned long long *nout) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nsys || ss[s].root < 0) return;
-  const unsigned long long slot = atomicAdd(nout, 1ull);
-  fout[slot] = make_int2(ss[s].root, ss[s].root);
+  if (s < nsys) fout[s] = make_int2(ss[s].root, ss[s].root);
+  if (s == 0) *nout = (unsigned long long)nsys;
 }
 
-__device__ __forceinline__ int64_t warp_incl_scan64(int64_t v, int lane) {
-#pragma unroll
-  for (int o = 1; o < kWarp; o <<= 1) {
-    const int64_t t = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= o) v += t;
-  }
+constexpr int kGenThreads = 256;            // one input pair per thread, one tile per block
+constexpr int kGenWarps = kGenThreads / kWarp;
+// tile words of the chained scan: top 2 bits the state, low 62 bits the count
+constexpr uint64_t kGenAggregate = 1ull << 62;  // the tile's own count
+constexpr uint64_t kGenInclusive = 2ull << 62;  // sum of the counts of tiles 0..t
+constexpr uint64_t kGenValue = (1ull << 62) - 1;
+constexpr int64_t kGenSpins = 1 << 22;          // per word; about a second at most
+
+__device__ __forceinline__ uint64_t gen_ld(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-
-// Reserves `cnt` slots for this lane in a list shared by the grid: one atomic
-// per warp on the list's counter.  Returns the lane's first slot, or -1 when
-// the warp's slots would pass `cap` (the list overflowed).
-__device__ __forceinline__ int64_t warp_reserve(unsigned long long *counter, int64_t cnt,
-                                                int64_t cap, int lane, unsigned long long *flags,
-                                                unsigned long long flag) {
-  const int64_t incl = warp_incl_scan64(cnt, lane);
-  const int64_t total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
-  int64_t base = 0;
-  if (lane == kWarp - 1 && total > 0) base = (int64_t)atomicAdd(counter, (unsigned long long)total);
-  base = __shfl_sync(0xffffffffu, base, kWarp - 1);
-  if (total == 0) return 0;
-  if (base + total > cap) {
-    if (lane == kWarp - 1) atomicOr(flags, flag);
-    return -1;
-  }
-  return base + incl - cnt;
+__device__ __forceinline__ void gen_st(uint64_t *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// One generation of the dual traversal.  Warps go through the input pairs 32
-// at a time; every lane classifies its pair, then the warp reserves the
-// output slots of all its lanes at once.
-__global__ void __launch_bounds__(256)
-dual_step_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *__restrict__ nin,
-                 int64_t cap_in, int2 *__restrict__ fout, unsigned long long *nout, int64_t cap_out,
-                 int2 *__restrict__ mut, unsigned long long *nmut, int64_t cap_mut, double theta2,
-                 unsigned long long *flags) {
+// Exclusive scan of one value per thread over the block; `ws` holds
+// kGenWarps ints; ends with a barrier so `ws` may be reused.
+__device__ __forceinline__ int gen_block_scan(int v, int *ws, int *total) {
+  const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == kWarp - 1) ws[warp] = x;
+  __syncthreads();
+  int before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < kGenWarps; ++w) {
+    const int c = ws[w];
+    if (w < warp) before += c;
+    all += c;
+  }
+  *total = all;
+  __syncthreads();
+  return before + x - v;
+}
+
+// Prefix of the counts of the tiles before tile t in one status list: publish
+// the tile's own count, then add up earlier tiles' words (an inclusive word
+// ends the walk).  Only tiles claimed earlier -- by blocks that are running
+// and publish before they wait -- are waited for, and every wait is bounded:
+// a wait that gives up raises kErrTimeout.
+__device__ __forceinline__ int64_t gen_lookback(uint64_t *status, int t, int64_t count,
+                                                int *err) {
+  uint64_t *word = status + t;
+  if (t == 0) {
+    gen_st(word, kGenInclusive | (uint64_t)count);
+    return 0;
+  }
+  gen_st(word, kGenAggregate | (uint64_t)count);
+  int64_t excl = 0;
+  int j = t - 1;
+  int64_t spins = 0;
+  while (j >= 0) {
+    const uint64_t w = gen_ld(status + j);
+    if ((w & ~kGenValue) == 0) {
+      if (++spins > kGenSpins) { atomicOr(err, kErrTimeout); break; }
+      continue;
+    }
+    excl += (int64_t)(w & kGenValue);
+    if ((w & ~kGenValue) == kGenInclusive) break;
+    --j;
+  }
+  gen_st(word, kGenInclusive | (uint64_t)(excl + count));
+  return excl;
+}
+
+// One generation of the dual traversal, as a deterministic compaction: block
+// tiles of kGenThreads input pairs are claimed in order from `tile_ctr`; every
+// thread classifies its pair, the block scans the counts of new frontier
+// pairs and of mutual pairs, and a chained scan over the tiles (separate
+// status words for the two lists) places every pair's outputs right after
+// those of the pairs before it.  So both lists come out in input order,
+// whatever the schedule: the frontier of the next generation, and the mutual
+// pairs appended after the `mut_base` written by earlier generations.  The
+// block of the last tile writes the two new totals (the next generation's
+// input count and the mutual count after this generation).
+__global__ void __launch_bounds__(kGenThreads)
+dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *__restrict__ nin,
+                int64_t cap_in, int2 *__restrict__ fout, unsigned long long *nout, int64_t cap_out,
+                int2 *__restrict__ mut, const unsigned long long *__restrict__ nmut_in,
+                unsigned long long *nmut_out, int64_t cap_mut, double theta2,
+                unsigned long long *flags, uint64_t *status_f, uint64_t *status_m,
+                int *tile_ctr, int *err) {
+  __shared__ int ws[kGenWarps];
+  __shared__ int s_tile;
+  __shared__ int64_t s_base[2];
   // after an overflow the count exceeds what was written: read only the buffer
-  const int64_t n_in = (int64_t)*nin < cap_in ? (int64_t)*nin : cap_in;
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); i0 < n_in;
-       i0 += stride) {
-    const int64_t i = i0 + lane;
+  const int64_t n_in = bh_min64((int64_t)*nin, cap_in);
+  const int64_t mut_base = (int64_t)*nmut_in;
+  const int64_t ntiles = (n_in + kGenThreads - 1) / kGenThreads;
+  if (ntiles == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *nout = 0; *nmut_out = (unsigned long long)mut_base; }
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1);
+    __syncthreads();
+    const int t = s_tile;
+    __syncthreads();
+    if ((int64_t)t >= ntiles) break;  // uniform across the block
+    const int64_t i = (int64_t)t * kGenThreads + threadIdx.x;
     // kind: 0 nothing, 1 children pairs of a self pair, 2 mutual, 3 open `o`
     int kind = 0, k = 0;
-    int64_t a = 0, b = 0, o = 0, other = 0;
+    int64_t a = -1, b = -1, o = 0, other = 0;
     bool open_a = false;
     int4 mt = make_int4(0, 0, 0, 0);
     if (i < n_in) {
       a = fin[i].x; b = fin[i].y;
+    }
+    if (a >= 0 && b >= 0) {
       const double4 ca = ent_com(e, a), cb = ent_com(e, b);
       if (ca.w != 0.0 && cb.w != 0.0) {
         if (a == b) {
@@ -176,37 +283,56 @@ dual_step_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *
         }
       }
     }
-    const int64_t n_out = kind == 1 ? (int64_t)k * (k + 1) / 2 : (kind == 3 ? k : 0);
-    const int64_t fo = warp_reserve(nout, n_out, cap_out, lane, flags, 1ull);
-    const int64_t mo = warp_reserve(nmut, kind == 2 ? 1 : 0, cap_mut, lane, flags, 2ull);
-    if (kind == 2 && mo >= 0) mut[mo] = make_int2((int)a, (int)b);
-    if (kind == 1 && fo >= 0) {
+    const int n_out = kind == 1 ? k * (k + 1) / 2 : (kind == 3 ? k : 0);
+    const int n_mut = kind == 2 ? 1 : 0;
+    int tot_f, tot_m;
+    const int off_f = gen_block_scan(n_out, ws, &tot_f);
+    const int off_m = gen_block_scan(n_mut, ws, &tot_m);
+    if (threadIdx.x == 0) {
+      const int64_t ef = gen_lookback(status_f, t, tot_f, err);
+      const int64_t em = gen_lookback(status_m, t, tot_m, err);
+      s_base[0] = ef;
+      s_base[1] = mut_base + em;
+      if ((int64_t)t == ntiles - 1) {
+        *nout = (unsigned long long)(ef + tot_f);
+        *nmut_out = (unsigned long long)(mut_base + em + tot_m);
+      }
+    }
+    __syncthreads();
+    const int64_t fo = s_base[0] + off_f, mo = s_base[1] + off_m;
+    if (n_out > 0 && fo + n_out > cap_out) atomicOr(flags, 1ull);
+    if (n_mut > 0 && mo + n_mut > cap_mut) atomicOr(flags, 2ull);
+    if (kind == 2 && mo < cap_mut) mut[mo] = make_int2((int)a, (int)b);
+    if (kind == 1 && fo + n_out <= cap_out) {
       int64_t w = fo;
       for (int p = 0; p < k; ++p) {
         const int64_t cp = node_child(e, a, mt, p);
         for (int q = p; q < k; ++q) fout[w++] = make_int2((int)cp, (int)node_child(e, a, mt, q));
       }
     }
-    if (kind == 3 && fo >= 0) {
+    if (kind == 3 && fo + n_out <= cap_out) {
       for (int q = 0; q < k; ++q) {
         const int64_t c = node_child(e, o, mt, q);
         fout[fo + q] = open_a ? make_int2((int)c, (int)other) : make_int2((int)other, (int)c);
       }
     }
+    __syncthreads();  // s_base is rewritten by the next tile
   }
 }
 
-// Both one-sided terms of every mutual pair, keyed (target << eb) | source.
+// Both one-sided terms of every mutual pair: key = target, value = source.
+// The mutual list is in a deterministic order, and the stable sort by target
+// keeps that order among a target's terms.
 __global__ void __launch_bounds__(256)
-expand_kernel(const int2 *__restrict__ mut, int64_t np, int eb, uint64_t *__restrict__ keys,
+expand_kernel(const int2 *__restrict__ mut, int64_t np, uint64_t *__restrict__ keys,
               int32_t *__restrict__ vals, int32_t *cnt) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t a = (uint32_t)mut[i].x, b = (uint32_t)mut[i].y;
-    keys[2 * (int64_t)i] = (a << eb) | b;
-    keys[2 * (int64_t)i + 1] = (b << eb) | a;
-    vals[2 * (int64_t)i] = 0;
-    vals[2 * (int64_t)i + 1] = 0;
+    const int32_t a = mut[i].x, b = mut[i].y;
+    keys[2 * (int64_t)i] = (uint64_t)(uint32_t)a;
+    vals[2 * (int64_t)i] = b;
+    keys[2 * (int64_t)i + 1] = (uint64_t)(uint32_t)b;
+    vals[2 * (int64_t)i + 1] = a;
     atomicAdd(&cnt[a], 1);
     atomicAdd(&cnt[b], 1);
   }
@@ -290,36 +416,47 @@ __device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 
   }
 }
 
-// Sum of the one-sided terms of every target, one warp per target: lane l
-// adds terms l, l + 32, ... of the target's source-ordered list, then the
-// lanes' sums are combined by a fixed butterfly, so the result depends only on
-// the target's own list.
+// Sum of the one-sided terms of every target, kEvalLanes lanes per target
+// (four targets per warp): lane l of a target's group adds terms l, l + 8, ...
+// of the target's list (in the mutual list's deterministic order), then the
+// group's sums are combined by a fixed butterfly, so the result depends only
+// on the target's own list.  Eight lanes rather than the whole warp: a target
+// has about a hundred terms, and a 19-value butterfly over 32 lanes per target
+// costs about a fifth of the evaluation.
+constexpr int kEvalLanes = 8;
+
 template <int ORDER>
 __global__ void __launch_bounds__(128)
-eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const uint64_t *__restrict__ keys,
-            int eb, double G, double eps2, double *__restrict__ F, double *__restrict__ H,
+eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const int32_t *__restrict__ src,
+            double G, double eps2, double *__restrict__ F, double *__restrict__ H,
             double *__restrict__ T) {
   constexpr int NV = ORDER >= 4 ? 19 : 3;
-  const uint64_t mask = (1ull << eb) - 1;
+  constexpr int kPerWarp = kWarp / kEvalLanes;
   const int lane = threadIdx.x & (kWarp - 1);
+  const int sub = lane / kEvalLanes, sl = lane % kEvalLanes;
+  const int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) / kWarp;
-  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; t < ne; t += wstride) {
+  for (int64_t t0 = warp_id * kPerWarp; t0 < ne; t0 += wstride * kPerWarp) {
+    const int64_t t = t0 + sub;
     double v[19];
 #pragma unroll
     for (int q = 0; q < 19; ++q) v[q] = 0.0;
-    const int kb = beg[t], ke = beg[t + 1];
-    if (kb < ke) {
-      const double4 ct = ent_com(e, t);
-      const bool tnode = t < e.n;
-      for (int k = kb + lane; k < ke; k += kWarp)
-        add_term<ORDER>(e, t, ct, tnode, (int64_t)(keys[k] & mask), G, eps2, v, v + 3, v + 9);
-#pragma unroll
-      for (int q = 0; q < NV; ++q) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[q] = v[q] + __shfl_xor_sync(0xffffffffu, v[q], o);
+    if (t < ne) {
+      const int kb = beg[t], ke = beg[t + 1];
+      if (kb < ke) {
+        const double4 ct = ent_com(e, t);
+        const bool tnode = t < e.n;
+        for (int k = kb + sl; k < ke; k += kEvalLanes)
+          add_term<ORDER>(e, t, ct, tnode, (int64_t)src[k], G, eps2, v, v + 3, v + 9);
       }
     }
-    if (lane == 0) {
+    // every lane of the warp takes part (lanes past ne hold zeros)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+#pragma unroll
+      for (int o = kEvalLanes / 2; o > 0; o >>= 1) v[q] = v[q] + __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (sl == 0 && t < ne) {
 #pragma unroll
       for (int q = 0; q < 3; ++q) F[3 * t + q] = v[q];
       if (ORDER >= 4) {
@@ -332,74 +469,82 @@ eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const uint64_t *
   }
 }
 
-// One level of the downward pass: every node of the level pushes its field,
-// hessian and third derivatives to its children.
-template <int ORDER>
-__global__ void __launch_bounds__(128)
-down_level_kernel(int level, const int32_t *__restrict__ level_begin, Ent e, double *F, double *H,
-                  double *T) {
-  const int lb = level_begin[level], le = level_begin[level + 1];
-  for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x) {
+// The node whose child a body is (a lone-particle child, or a body of a
+// node of identical keys), for every sorted position.
+__global__ void __launch_bounds__(256)
+body_parent_kernel(const Scalars *__restrict__ scr, Ent e, int32_t *__restrict__ bp) {
+  const int M = scr->n_compact;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
     const int4 mt = e.meta[j];
-    const double4 cj = e.com[j];
-    const double Fx = F[3 * j], Fy = F[3 * j + 1], Fz = F[3 * j + 2];
-    double h[6], t[10];
-    if (ORDER >= 4) {
-#pragma unroll
-      for (int q = 0; q < 6; ++q) h[q] = H[6 * (int64_t)j + q];
-#pragma unroll
-      for (int q = 0; q < 10; ++q) t[q] = T[10 * (int64_t)j + q];
-    }
-    const int k = node_nchild(mt);
-    for (int q = 0; q < k; ++q) {
-      const int64_t c = node_child(e, j, mt, q);
-      const double4 cc = ent_com(e, c);
-      if (cc.w == 0.0) continue;
-      double fx = F[3 * c] + Fx, fy = F[3 * c + 1] + Fy, fz = F[3 * c + 2] + Fz;
-      if (ORDER >= 4) {
-        const double dx = cc.x - cj.x, dy = cc.y - cj.y, dz = cc.z - cj.z;
-        const double hxx = h[0], hyy = h[1], hzz = h[2], hxy = h[3], hxz = h[4], hyz = h[5];
-        const double txxx = t[0], txxy = t[1], txxz = t[2], txyy = t[3], txyz = t[4], txzz = t[5],
-                     tyyy = t[6], tyyz = t[7], tyzz = t[8], tzzz = t[9];
-        fx = fx + hxx * dx + hxy * dy + hxz * dz + txxy * dx * dy + txxz * dx * dz + txyz * dy * dz +
-             0.5 * (txxx * dx * dx + txyy * dy * dy + txzz * dz * dz);
-        fy = fy + hxy * dx + hyy * dy + hyz * dz + txyy * dx * dy + txyz * dx * dz + tyyz * dy * dz +
-             0.5 * (txxy * dx * dx + tyyy * dy * dy + tyzz * dz * dz);
-        fz = fz + hxz * dx + hyz * dy + hzz * dz + txyz * dx * dy + txzz * dx * dz + tyzz * dy * dz +
-             0.5 * (txxz * dx * dx + tyyz * dy * dy + tzzz * dz * dz);
-        if (c < e.n) {
-          double *hc = H + 6 * c;
-          hc[0] = hc[0] + hxx + txxx * dx + txxy * dy + txxz * dz;
-          hc[1] = hc[1] + hyy + txyy * dx + tyyy * dy + tyyz * dz;
-          hc[2] = hc[2] + hzz + txzz * dx + tyzz * dy + tzzz * dz;
-          hc[3] = hc[3] + hxy + txxy * dx + txyy * dy + txyz * dz;
-          hc[4] = hc[4] + hxz + txxz * dx + txyz * dy + txzz * dz;
-          hc[5] = hc[5] + hyz + txyz * dx + tyyz * dy + tyzz * dz;
-          double *tc = T + 10 * c;
-#pragma unroll
-          for (int r = 0; r < 10; ++r) tc[r] = tc[r] + t[r];
-        }
+    if (mt.w == 0) {
+      for (int c = 0; c < mt.y; ++c) bp[mt.x + c] = j;
+    } else {
+      for (int c = 0; c < mt.w; ++c) {
+        const int32_t ch = e.child[8 * (int64_t)j + c];
+        if (ch < 0) bp[~ch] = j;
       }
-      F[3 * c] = fx; F[3 * c + 1] = fy; F[3 * c + 2] = fz;
     }
   }
 }
 
-// Forces in the original order, one (n_s, 3) Fortran block per system.
-__global__ void __launch_bounds__(256)
-dehnen_out_kernel(int64_t n, const double *__restrict__ F, const double4 *__restrict__ spos,
-                  const int32_t *__restrict__ perm, const int32_t *__restrict__ sys_of,
-                  const SysScalars *__restrict__ ss, int out_kind, double *__restrict__ out) {
+// The downward pass (dehnen_forces, octree_default.f90:1560-1673) and the
+// output in one launch, one thread per body.  The pass adds to every child
+// the parent's field translated to the child's centre of mass (F + H d +
+// d.T.d / 2, H + T d, T), so a body ends with the sum of every ancestor's own
+// expansion translated to it; the translation of a cubic-potential expansion
+// is exact, so the body sums its ancestors' translations directly, from the
+// root down, instead of waiting for the levels above it.  A massless body
+// receives nothing (the pass skips massless children).  The force is m times
+// the field; forces go out in the original order, one (n_s, 3) Fortran block
+// per system.  A parent chain longer than the deepest tree raises kErrIndex.
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+down_bodies_kernel(int64_t n, Ent e, const int32_t *__restrict__ bp,
+                   const int32_t *__restrict__ parent, const double *__restrict__ F,
+                   const double *__restrict__ H, const double *__restrict__ T,
+                   const int32_t *__restrict__ perm, const int32_t *__restrict__ sys_of,
+                   const SysScalars *__restrict__ ss, int out_kind, double *__restrict__ out,
+                   int *err) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
+    const double4 cb = e.spos[p];
+    const double *fl = F + 3 * (n + p);
+    double fx = fl[0], fy = fl[1], fz = fl[2];
     const SysScalars &s = ss[sys_of[p]];
-    const double sc = out_kind == 0 ? spos[p].w : 1.0;
+    if (cb.w != 0.0 && s.root >= 0) {
+      int chain[kNumLevels + 2];
+      int depth = 0;
+      bool ok = true;
+      for (int j = bp[p]; j >= 0; j = parent[j]) {
+        if (depth >= kNumLevels + 2) { ok = false; break; }
+        chain[depth++] = j;
+      }
+      if (!ok) atomicOr(err, kErrIndex);
+      for (int k = ok ? depth - 1 : -1; k >= 0; --k) {
+        const int j = chain[k];
+        fx += F[3 * (int64_t)j]; fy += F[3 * (int64_t)j + 1]; fz += F[3 * (int64_t)j + 2];
+        if (ORDER >= 4) {
+          const double4 cj = e.com[j];
+          const double dx = cb.x - cj.x, dy = cb.y - cj.y, dz = cb.z - cj.z;
+          const double *h = H + 6 * (int64_t)j, *t = T + 10 * (int64_t)j;
+          const double hxx = h[0], hyy = h[1], hzz = h[2], hxy = h[3], hxz = h[4], hyz = h[5];
+          const double txxx = t[0], txxy = t[1], txxz = t[2], txyy = t[3], txyz = t[4],
+                       txzz = t[5], tyyy = t[6], tyyz = t[7], tyzz = t[8], tzzz = t[9];
+          fx += hxx * dx + hxy * dy + hxz * dz + txxy * dx * dy + txxz * dx * dz + txyz * dy * dz +
+                0.5 * (txxx * dx * dx + txyy * dy * dy + txzz * dz * dz);
+          fy += hxy * dx + hyy * dy + hyz * dz + txyy * dx * dy + txyz * dx * dz + tyyz * dy * dz +
+                0.5 * (txxy * dx * dx + tyyy * dy * dy + tyzz * dz * dz);
+          fz += hxz * dx + hyz * dy + hzz * dz + txyz * dx * dy + txzz * dx * dz + tyzz * dy * dz +
+                0.5 * (txxz * dx * dx + tyyz * dy * dy + tzzz * dz * dz);
+        }
+      }
+    }
+    const double sc = out_kind == 0 ? cb.w : 1.0;
     const int64_t o = perm[p] - s.off;
     double *base = out + 3 * s.off;
-    const double *f = F + 3 * (n + p);
-    base[o] = sc * f[0];
-    base[s.n + o] = sc * f[1];
-    base[2 * s.n + o] = sc * f[2];
+    base[o] = sc * fx;
+    base[s.n + o] = sc * fy;
+    base[2 * s.n + o] = sc * fz;
   }
 }
 
@@ -424,7 +569,7 @@ int bits_for64(int64_t v) {
 
 void free_dehnen(DehnenBuffers &d) {
   void *ptrs[] = {d.rmax, d.F, d.H, d.T, d.front, d.mut, d.keys, d.vals, d.cnt, d.beg, d.hist,
-                  d.scan_tmp, d.counters};
+                  d.scan_tmp, d.counters, d.gen_status, d.gen_tiles};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   d = DehnenBuffers();
@@ -447,34 +592,42 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
   Ent e;
   e.meta = b.cn_meta; e.child = b.cn_child; e.com = b.cn_com; e.spos = b.spos;
   e.quad = b.cn_quad; e.oct = b.cn_oct; e.rmax = d.rmax; e.n = n;
-  const int lgrid = grid_for(n / 2 + 1, 128, 148 * 8);
-  for (int level = kMaxDepth; level >= 0; --level)
-    rmax_level_kernel<<<lgrid, 128, 0, s>>>(level, b.level_begin, e, d.rmax);
+  const int lgrid = grid_for(n / 2 + 1, 256, 148 * 8);
+  cudaMemsetAsync(d.cnt, 0, (ne + 1) * sizeof(int32_t), s);  // arrival counters (M < ne)
+  rmax_fused_kernel<<<lgrid, 256, 0, s>>>(b.sc, e, b.cn_parent, d.rmax, d.cnt, &b.sc->err);
 
-  const int eb = bits_for64(ne);
-  // counters: [0], [1] frontier sizes, [2] mutual pairs, [3] overflow flags
-  unsigned long long *cnt_front = d.counters;
-  unsigned long long h[4] = {0, 0, 0, 0};
+  // counters: [0], [1] frontier sizes and [2], [3] mutual totals, each
+  // alternating between generations; [4] overflow flags
+  unsigned long long *cnt = d.counters;
+  unsigned long long h[5] = {0, 0, 0, 0, 0};
+  if (b.nsys > 16 * n) return 4;
   for (int attempt = 0; attempt < 8; ++attempt) {
     if (grow(d.front, d.front_cap, 2 * d.want_front) != cudaSuccess) return 1;
     if (grow(d.mut, d.mut_cap, d.want_mut) != cudaSuccess) return 1;
     int2 *f0 = d.front, *f1 = d.front + d.front_cap / 2;
     const int64_t fcap = d.front_cap / 2;
+    const int64_t max_tiles = fcap / kGenThreads + 1;  // tiles of one generation's input
+    if (grow(d.gen_status, d.gen_status_cap, (int64_t)kGenerations * 2 * max_tiles) != cudaSuccess)
+      return 1;
+    if (grow(d.gen_tiles, d.gen_tiles_cap, (int64_t)kGenerations) != cudaSuccess) return 1;
     cudaMemsetAsync(d.counters, 0, 8 * sizeof(unsigned long long), s);
-    roots_frontier_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, f0, cnt_front);
+    cudaMemsetAsync(d.gen_status, 0, (size_t)kGenerations * 2 * max_tiles * sizeof(uint64_t), s);
+    cudaMemsetAsync(d.gen_tiles, 0, kGenerations * sizeof(int32_t), s);
+    roots_frontier_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, f0, cnt);
     for (int g = 0; g < kGenerations; ++g) {
       int2 *fi = (g & 1) ? f1 : f0, *fo = (g & 1) ? f0 : f1;
-      unsigned long long *ni = cnt_front + (g & 1), *no = cnt_front + ((g + 1) & 1);
-      cudaMemsetAsync(no, 0, sizeof(unsigned long long), s);
-      dual_step_kernel<<<148 * 8, 256, 0, s>>>(e, fi, ni, fcap, fo, no, fcap, d.mut, cnt_front + 2,
-                                               d.mut_cap, p.theta2, cnt_front + 3);
+      uint64_t *st = d.gen_status + (int64_t)g * 2 * max_tiles;
+      dual_gen_kernel<<<148 * 8, kGenThreads, 0, s>>>(
+          e, fi, cnt + (g & 1), fcap, fo, cnt + ((g + 1) & 1), fcap, d.mut, cnt + 2 + (g & 1),
+          cnt + 2 + ((g + 1) & 1), d.mut_cap, p.theta2, cnt + 4, st, st + max_tiles,
+          d.gen_tiles + g, &b.sc->err);
     }
-    if (cudaMemcpyAsync(h, d.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    if (cudaMemcpyAsync(h, d.counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                         s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
       return 2;
-    if (h[3] & 4) return 3;
-    const bool more_front = (h[3] & 1) != 0, more_mut = (h[3] & 2) != 0;
+    if (h[4] & 4) return 3;
+    const bool more_front = (h[4] & 1) != 0, more_mut = (h[4] & 2) != 0;
     if (!more_front && !more_mut) {
       if (h[kGenerations & 1] != 0) return 3;  // the traversal did not close
       break;
@@ -484,7 +637,7 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
     if (more_mut) d.want_mut *= 2;
     if (d.want_mut > ((int64_t)1 << 30) || d.want_front > ((int64_t)1 << 30)) return 4;
   }
-  const int64_t np = (int64_t)h[2];
+  const int64_t np = (int64_t)h[2 + (kGenerations & 1)];
   const int64_t nh = 2 * np;
   if (grow(d.keys, d.keys_cap, 2 * (nh > 0 ? nh : 1)) != cudaSuccess) return 1;
   if (grow(d.vals, d.vals_cap, 2 * (nh > 0 ? nh : 1)) != cudaSuccess) return 1;
@@ -492,27 +645,31 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
   cudaMemsetAsync(d.cnt, 0, (ne + 1) * sizeof(int32_t), s);
   if (np > 0) {
     const int g = grid_for(np, 256, 148 * 16);
-    expand_kernel<<<g, 256, 0, s>>>(d.mut, np, eb, d.keys, d.vals, d.cnt);
-    radix_sort_pairs(d.keys, d.vals, d.keys + nh, d.vals + nh, nh, nullptr, 2 * eb, d.hist,
+    expand_kernel<<<g, 256, 0, s>>>(d.mut, np, d.keys, d.vals, d.cnt);
+    // stable by target: a target's terms keep the mutual list's order
+    radix_sort_pairs(d.keys, d.vals, d.keys + nh, d.vals + nh, nh, nullptr, bits_for64(ne), d.hist,
                      &b.sc->err, s);
   }
-  exclusive_scan(d.cnt, d.beg, ne + 1, nullptr, nullptr, d.scan_tmp, s);
-  const int egrid = grid_for(ne * kWarp, 128, 148 * 32);
+  exclusive_scan(d.cnt, d.beg, ne + 1, nullptr, nullptr, d.scan_tmp, &b.sc->err, s);
+  const int egrid = grid_for(ne * kEvalLanes, 128, 148 * 32);
   const double G = p.G, eps2 = p.eps2;
   if (p.order >= 8)
-    eval_kernel<8><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.keys, eb, G, eps2, d.F, d.H, d.T);
+    eval_kernel<8><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
   else if (p.order >= 4)
-    eval_kernel<4><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.keys, eb, G, eps2, d.F, d.H, d.T);
+    eval_kernel<4><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
   else
-    eval_kernel<1><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.keys, eb, G, eps2, d.F, d.H, d.T);
-  for (int level = 0; level <= kMaxDepth; ++level) {
-    if (p.order >= 4)
-      down_level_kernel<4><<<lgrid, 128, 0, s>>>(level, b.level_begin, e, d.F, d.H, d.T);
-    else
-      down_level_kernel<1><<<lgrid, 128, 0, s>>>(level, b.level_begin, e, d.F, d.H, d.T);
-  }
-  dehnen_out_kernel<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(n, d.F, b.spos, b.v0, b.sys_of,
-                                                                 b.ss, p.out_kind, out);
+    eval_kernel<1><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
+  // downward pass and output: every body sums its ancestors' translated
+  // expansions (cnt is free after the scan: it holds each body's parent node)
+  int32_t *bp = d.cnt;
+  body_parent_kernel<<<lgrid, 256, 0, s>>>(b.sc, e, bp);
+  const int bgrid = grid_for(n, 128, 148 * 16);
+  if (p.order >= 4)
+    down_bodies_kernel<4><<<bgrid, 128, 0, s>>>(n, e, bp, b.cn_parent, d.F, d.H, d.T, b.v0,
+                                                 b.sys_of, b.ss, p.out_kind, out, &b.sc->err);
+  else
+    down_bodies_kernel<1><<<bgrid, 128, 0, s>>>(n, e, bp, b.cn_parent, d.F, d.H, d.T, b.v0,
+                                                 b.sys_of, b.ss, p.out_kind, out, &b.sc->err);
   d.pairs = np;
   return 0;
 }

@@ -149,16 +149,18 @@ inline int grid_for(int64_t n, int threads, int cap) {
 // kErrTimeout in *err (device).
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
                       const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s);
-// scratch of the radix sort, in int32 entries: digit counts of 8 passes x 256
+// scratch of the scan, in int32 entries: a ticket and a 64-bit word per
+// 8192-value tile; scratch of the radix sort: digit counts of 8 passes x 256
 // digits, 8 tile counters, and a 64-bit word per (pass, 4096-key tile, digit)
-constexpr int64_t scan_tmp_entries(int64_t n) { return (n + 8191) / 8192 + 2; }
+constexpr int64_t scan_tmp_entries(int64_t n) { return 2 * ((n + 8191) / 8192) + 4; }
 constexpr int64_t radix_hist_entries(int64_t n) {
   return 8 * 256 + 8 + 2 * 8 * 256 * ((n + 4095) / 4096 + 1);
 }
 
-// exclusive scan of n int32 values; total written to *total (device) if given
+// exclusive scan of n int32 values in one launch; total written to *total
+// (device) if given; a look-back wait that gives up sets kErrTimeout in *err
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
-                    int32_t *total, int32_t *tmp, cudaStream_t s);
+                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s);
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s);
@@ -199,6 +201,10 @@ struct DehnenBuffers {
   unsigned long long *counters = nullptr;
   int64_t keys_cap = 0, vals_cap = 0, cnt_cap = 0, beg_cap = 0, hist_cap = 0, scan_tmp_cap = 0,
           counters_cap = 0;
+  uint64_t *gen_status = nullptr;         // chained-scan words of every traversal generation
+  int64_t gen_status_cap = 0;
+  int32_t *gen_tiles = nullptr;           // tile tickets, one counter per generation
+  int64_t gen_tiles_cap = 0;
   int64_t pairs = 0;                      // mutual interactions of the last run
 };
 // Dehnen's method over the built batch into out (same layout as the walk).

@@ -232,57 +232,65 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
 
 // ---- exclusive scan ----
 
+// Single-pass exclusive scan (chained scan with decoupled look-back): block b
+// claims tile t (kScanChunk values) from a ticket, sums it, publishes the sum,
+// adds up the earlier tiles' words (an inclusive word ends the walk), then
+// writes its outputs.  A block only waits for tiles claimed before its own by
+// blocks that are running and publish before they wait; every wait is
+// bounded and one that gives up raises kErrTimeout in *err.
+// tmp (int32 entries): [0] ticket, [1] unused, then one 64-bit word per tile.
 __global__ void __launch_bounds__(kScanThreads)
-scan_reduce_kernel(const int32_t *__restrict__ in, int64_t n_max, const int32_t *n_dev,
-                   int32_t *__restrict__ block_sums) {
+scan_onepass_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n_max,
+                    const int32_t *n_dev, int32_t *tmp, int32_t *total_out, int *err) {
   __shared__ int ws[kScanThreads / kWarp];
+  __shared__ int s_tile;
+  __shared__ int64_t s_excl;
+  if (threadIdx.x == 0) s_tile = atomicAdd(tmp, 1);
+  __syncthreads();
+  const int t = s_tile;
   const int64_t n = n_dev ? bh_min64(n_max, (int64_t)*n_dev) : n_max;
-  const int64_t base = (int64_t)blockIdx.x * kScanChunk + (int64_t)threadIdx.x * kScanItems;
-  int s = 0;
-#pragma unroll
-  for (int i = 0; i < kScanItems; ++i)
-    if (base + i < n) s += in[base + i];
-  int total;
-  block_excl_scan(s, ws, &total);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kScanThreads)
-scan_blocks_kernel(int32_t *block_sums, int nb, int32_t *total_out) {
-  __shared__ int ws[kScanThreads / kWarp];
-  int carry = 0;
-  for (int base = 0; base < nb; base += kScanThreads) {
-    int i = base + threadIdx.x;
-    int v = i < nb ? block_sums[i] : 0;
-    int tot;
-    int ex = block_excl_scan(v, ws, &tot);
-    if (i < nb) block_sums[i] = carry + ex;
-    carry += tot;
-  }
-  if (threadIdx.x == 0) {
-    block_sums[nb] = carry;
-    if (total_out) *total_out = carry;
-  }
-}
-
-__global__ void __launch_bounds__(kScanThreads)
-scan_apply_kernel(const int32_t *in, int32_t *out, int64_t n_max, const int32_t *n_dev,
-                  const int32_t *__restrict__ block_sums) {
-  __shared__ int ws[kScanThreads / kWarp];
-  const int64_t n = n_dev ? bh_min64(n_max, (int64_t)*n_dev) : n_max;
-  const int64_t base = (int64_t)blockIdx.x * kScanChunk + (int64_t)threadIdx.x * kScanItems;
+  const int64_t ntiles = n > 0 ? (n + kScanChunk - 1) / kScanChunk : 1;
+  if ((int64_t)t >= ntiles) return;  // uniform across the block
+  uint64_t *words = reinterpret_cast<uint64_t *>(tmp + 2);
+  const int64_t base = (int64_t)t * kScanChunk + (int64_t)threadIdx.x * kScanItems;
   int vals[kScanItems];
-  int s = 0;
+  int sum = 0;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
     vals[i] = (base + i < n) ? in[base + i] : 0;
-    s += vals[i];
+    sum += vals[i];
   }
-  int off = block_excl_scan(s, ws, nullptr) + block_sums[blockIdx.x];
+  int tile_total;
+  int off = block_excl_scan(sum, ws, &tile_total);
+  if (threadIdx.x == 0) {
+    int64_t excl = 0;
+    if (t == 0) {
+      st_relaxed(words, kTileInclusive | (uint64_t)tile_total);
+    } else {
+      st_relaxed(words + t, kTileAggregate | (uint64_t)tile_total);
+      int j = t - 1;
+      int64_t spins = 0;
+      while (j >= 0) {
+        const uint64_t w = ld_relaxed(words + j);
+        if ((w & ~kTileValue) == 0) {
+          if (++spins > kLookbackSpins) { atomicOr(err, kErrTimeout); break; }
+          continue;
+        }
+        excl += (int64_t)(w & kTileValue);
+        if ((w & ~kTileValue) == kTileInclusive) break;
+        --j;
+      }
+      st_relaxed(words + t, kTileInclusive | (uint64_t)(excl + tile_total));
+    }
+    s_excl = excl;
+    if ((int64_t)t == ntiles - 1 && total_out) *total_out = (int32_t)(excl + tile_total);
+  }
+  __syncthreads();
+  int64_t o = s_excl + off;
 #pragma unroll
   for (int i = 0; i < kScanItems; ++i) {
-    if (base + i < n) out[base + i] = off;
-    off += vals[i];
+    if (base + i < n) out[base + i] = (int32_t)o;
+    o += vals[i];
   }
 }
 
@@ -328,12 +336,11 @@ static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256 && kMaxPasses
               "scan_tmp_entries / radix_hist_entries in bh_internal.cuh assume these sizes");
 
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
-                    int32_t *total, int32_t *tmp, cudaStream_t s) {
+                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s) {
   int nb = (int)((n + kScanChunk - 1) / kScanChunk);
   if (nb < 1) nb = 1;
-  scan_reduce_kernel<<<nb, kScanThreads, 0, s>>>(in, n, n_dev, tmp);
-  scan_blocks_kernel<<<1, kScanThreads, 0, s>>>(tmp, nb, total);
-  scan_apply_kernel<<<nb, kScanThreads, 0, s>>>(in, out, n, n_dev, tmp);
+  cudaMemsetAsync(tmp, 0, (2 + 2 * (int64_t)nb) * sizeof(int32_t), s);
+  scan_onepass_kernel<<<nb, kScanThreads, 0, s>>>(in, out, n, n_dev, tmp, total, err);
 }
 
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,

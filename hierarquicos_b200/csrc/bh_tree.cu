@@ -269,7 +269,7 @@ void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s) {
   // rank of each marked node in binary order, total -> n_compact
   int32_t *rank = b.gscan;          // free until the group pass
   int32_t *total = b.counters + 2;  // scratch counter
-  exclusive_scan(b.bn_flag, rank, n, nullptr, total, b.scan_tmp, s);
+  exclusive_scan(b.bn_flag, rank, n, nullptr, total, b.scan_tmp, &b.sc->err, s);
   count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 0);
   // sort the compact nodes by (level, first particle)
   const int first_bits = bits_for(n);
@@ -297,7 +297,7 @@ void launch_groups(int64_t n, int group_size, int group_span, Buffers &b, cudaSt
                                           group_span, b.gflag);
   system_starts_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, b.gflag);
   int32_t *total = b.counters + 3;
-  exclusive_scan(b.gflag, b.gscan, n, nullptr, total, b.scan_tmp, s);
+  exclusive_scan(b.gflag, b.gscan, n, nullptr, total, b.scan_tmp, &b.sc->err, s);
   count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 1);
   group_first_kernel<<<grid, 256, 0, s>>>(n, b.gflag, b.gscan, b.sc, b.g_first);
 }
