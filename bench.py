@@ -30,12 +30,13 @@ ones.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
   python bench.py --serving-sweep     # the serving config: Poisson arrivals, rate swept
+  python bench.py --parareal          # the batched Parareal config
 
 One process per GPU (torchrun for N > 1): every rank serves its own systems
 (weak scaling, no collective on the data path); times are the max over
 ranks.  ``--impl reference`` times the CPU restatement of the reference's
 Fortran (the reference cannot be compiled here: no Fortran compiler) on this
-host's cores.
+host's cores: one full force evaluation of the headline system per step.
 """
 from __future__ import annotations
 
@@ -113,6 +114,11 @@ def parse():
                          "rate swept, force and leapfrog requests, N log-uniform in [1024, 2^21] "
                          "over three profiles); prints one JSON line of its own")
     ap.add_argument("--sweep-requests", type=int, default=48)
+    ap.add_argument("--parareal", action="store_true",
+                    help="instead of the headline line: the batched Parareal config (Plummer "
+                         "16384, 64 slices, coarse monopole theta 0.8, fine quadrupole theta 0.3)")
+    ap.add_argument("--parareal-bodies", type=int, default=16384)
+    ap.add_argument("--parareal-iters", type=int, default=24)
     ap.add_argument("--no-extras", action="store_true",
                     help="plain timed calls only (no serving, error check, e2e, batch or CPU baseline)")
     return ap.parse_args()
@@ -294,17 +300,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 walk (Kahan), f64 keys/moments",
             "data": "synthetic (seeded Hernquist ICs drawn on the device)",
-            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, force requests",
-                       "n_per_request": n, "requests_per_gpu": K, "theta": THETA, "eps": EPS,
-                       "order": args.order,
-                       "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk",
-                                2: "fp64 per-target", 3: "fp64 dehnen dual tree"}[args.precision],
-                       "group_size": args.group_size, "leaf_cap": args.leaf_cap,
-                       "group_span": args.group_span or 2 * args.group_size, "mac": p.mac, "pipeline": p.pipeline,
-                       "keys": "63-bit, strict",
-                       "l2": "plain: flushed (256 MiB write) before every call; served: every request "
-                             "touches > 500 MB of distinct data (inputs larger than L2)",
-                       "parallelism": f"independent systems per rank x{world}"},
+            "config": headline_config(args, n, p.mac, p.pipeline, K, world),
             "plain": {"value": plain_value, "unit": "forces/s", "ms_per_step": plain_ms,
                       "phases_ms": {"build": statistics.mean(t_build),
                                     "walk": statistics.mean(t_walk),
@@ -482,6 +478,28 @@ def run_ours(args):
             b.synchronize()
             te.append(a.elapsed_time(b))
         plain_e2e_ms = dist_max(statistics.mean(te), dev, world)
+        # the api3d drop-in from ordinary (pageable) numpy arrays, as the
+        # reference's f2py callers pass them: a fresh Fortran-ordered result
+        # array per call, as the f2py function returns
+        from hierarquicos_b200 import api3d
+
+        pm, px_, py_, pz_ = (h.numpy().copy() for h in (hm, hx, hy, hz))
+        for _ in range(W):
+            api3d.compute_forces(pm, px_, py_, pz_, THETA, 1.0, EPS, order=args.order, mac=p.mac,
+                                 pipeline=p.pipeline)
+        tp = []
+        for _ in range(K):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            api3d.compute_forces(pm, px_, py_, pz_, THETA, 1.0, EPS, order=args.order, mac=p.mac,
+                                 pipeline=p.pipeline)
+            b.record(stream)
+            b.synchronize()
+            tp.append(a.elapsed_time(b))
+        pageable_ms = dist_max(statistics.mean(tp), dev, world)
         host_sys = []
         for i in range(K + W):
             mm, xx, yy, zz = systems[i]
@@ -501,15 +519,18 @@ def run_ours(args):
                        "p50_ms": hmet["p50_ms"], "p99_ms": hmet["p99_ms"],
                        "equal_to_plain_bitwise": same_host,
                        "plain": {"value": world * n / (plain_e2e_ms * 1e-3), "ms_per_step": plain_e2e_ms,
-                                 "api": "bh_compute_forces_ex (host arrays, the api3d drop-in)"}}
+                                 "api": "bh_compute_forces_ex (pinned host arrays)"},
+                       "plain_pageable": {"value": world * n / (pageable_ms * 1e-3),
+                                          "ms_per_step": pageable_ms,
+                                          "api": "api3d.compute_forces (pageable numpy arrays in, "
+                                                 "a new (N,3) Fortran array out)"}}
         del systems, host_sys, hreqs, hwarm, reqs
 
         # ---- 512 independent systems: batched vs plain loop ----
         line["batched"] = bench_batch(args, p, dev, local, world, rank)
 
         if rank == 0 and world == 1:
-            m0, q0 = workload(n, seed=1000)
-            line["cpu_baseline"] = cpu_baseline(n, m0, q0, args.order, samples=32768)
+            line["cpu_baseline"] = cpu_baseline(n, args.order)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -676,58 +697,91 @@ def bench_batch(args, p, dev, local, world, rank):
             "unit": "forces/s"}
 
 
-def cpu_baseline(n, m, q, order, samples):
-    """CPU restatement of the reference (morton_octree.f90 keys/sort/build/
-    quadrupole + barnes_hut walk) on this host's cores: the full tree build
-    plus the walk of a seeded sample of targets, scaled to all N targets."""
-    import oracle
+def cpu_baseline_runs(n, order, runs, warmup, seed=1000):
+    """The CPU restatement of the reference's Morton path (morton_octree.f90:
+    init = keys, merge sort, node build, quadrupole upward pass; forces_par =
+    the per-target barnes_hut walk of all N bodies under OpenMP), built with
+    the reference's flags (-O3 -march=native -fopenmp) for this host, run in a
+    child process on all usable cores with OMP_PROC_BIND=close: ``warmup`` +
+    ``runs`` full force evaluations of the seeded Hernquist system.  Returns the
+    summary with the per-run times."""
+    from oracle.cpu_baseline import child_env, usable_cores
 
-    x, y, z = (np.ascontiguousarray(q[:, k]) for k in range(3))
-    t0 = time.perf_counter()
-    tree = oracle.MortonTree(m, x, y, z, L=21, ssa=1.2, use_quadrupole=order >= 4, fma_mode=1)
-    t_build = time.perf_counter() - t0
-    rng = np.random.default_rng(7)
-    samples = min(samples, n)
-    tg = rng.choice(n, samples, replace=False)
-    t0 = time.perf_counter()
-    tree.forces_targets(tg, 1.0, EPS * EPS, THETA * THETA, order >= 4)
-    t_walk = time.perf_counter() - t0
-    total = t_build + t_walk * n / samples
-    del tree
-    return {"value": n / total, "unit": "forces/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"full 1M tree build ({t_build:.2f} s) + walk of {samples} seeded targets "
-                      f"({t_walk:.2f} s) scaled to N",
-            "build_s": t_build, "walk_s_scaled": t_walk * n / samples}
+    cores = usable_cores()
+    r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n), "--runs",
+                        str(runs), "--warmup", str(warmup), "--order", str(order), "--seed",
+                        str(seed), "--theta", str(THETA), "--eps", str(EPS)],
+                       env=child_env(cores), cwd=ROOT, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"CPU baseline failed ({r.returncode}): {r.stderr[-2000:]}")
+    for line in r.stdout.splitlines()[::-1]:
+        if line.startswith('{"summary"'):
+            return json.loads(line)["summary"]
+    raise RuntimeError("CPU baseline printed no summary")
+
+
+def cpu_baseline(n, order, runs=3, warmup=1):
+    """``cpu_baseline`` object of the bench line: the median of ``runs`` full
+    force evaluations on the host's cores (about 4-5 s each at N = 2^20 on 16
+    cores), nothing extrapolated."""
+    sm = cpu_baseline_runs(n, order, runs, warmup)
+    return {"value": n / sm["median_total_s"], "unit": "forces/s", "cores": sm["threads"],
+            "kind": "port",
+            "sample": f"{runs} full force evaluations of N={n} (after {warmup} warm-up): tree build "
+                      f"(serial, as morton_octree.f90 generate_nodes) + per-target walk of all N "
+                      f"targets (OpenMP); median; -O3 -march=native -fopenmp build of the oracle",
+            "build_s": sm["median_build_s"], "walk_s": sm["median_walk_s"],
+            "per_run_s": sm["per_run_s"]}
+
+
+def headline_config(args, n, mac, pipeline, K, world):
+    """The bench line's ``config``: the same object for both arms."""
+    return {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, force requests",
+            "n_per_request": n, "requests_per_gpu": K, "theta": THETA, "eps": EPS,
+            "order": args.order,
+            "walk": {0: "fp32-kahan group walk", 1: "fp64 group walk",
+                     2: "fp64 per-target", 3: "fp64 dehnen dual tree"}[args.precision],
+            "group_size": args.group_size, "leaf_cap": args.leaf_cap,
+            "group_span": args.group_span or 2 * args.group_size, "mac": mac,
+            "pipeline": pipeline, "keys": "63-bit, strict",
+            "l2": "plain: flushed (256 MiB write) before every call; served: every request "
+                  "touches > 500 MB of distinct data (inputs larger than L2)",
+            "parallelism": f"independent systems per rank x{world}"}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's Fortran path,
+    timed on this host's cores (the reference itself is Fortran and no Fortran
+    compiler exists on these hosts).  Every step is one full force evaluation
+    of the headline system (tree build + walk of all N targets); W warm-up
+    steps, then exactly K timed ones.  Under torchrun only rank 0 runs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle
-
-    oracle.build()
     n = args.n
-    m, q = workload(n, seed=1000)
-    samples = 8192
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(n, m, q, args.order, samples)
-        if i >= args.warmup:
-            vals.append(cb)
-    value = statistics.mean(v["value"] for v in vals)
+    sm = cpu_baseline_runs(n, args.order, args.steps, args.warmup)
+    step_s = sm["mean_total_s"]
+    value = n / step_s
+    from hierarquicos_b200._lib import default_params
+
+    p = default_params()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "forces/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * n / value, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * step_s, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Hernquist ICs)",
-            "config": {"workload": f"hernquist N={n} a=1 r<=100a equal masses seeded, force requests",
-                       "n_per_request": n, "theta": THETA, "eps": EPS, "order": args.order},
-            "cpu_baseline": {"value": value, "unit": "forces/s", "cores": vals[0]["cores"],
+            "config": headline_config(args, n, args.mac if args.mac is not None else p.mac,
+                                      args.pipeline if args.pipeline is not None else p.pipeline,
+                                      args.steps, world),
+            "reference_path": "CPU restatement of morton_octree.f90 init + forces_par "
+                              "(per-target barnes_hut walk, FP64), -O3 -march=native -fopenmp",
+            "cpu_baseline": {"value": value, "unit": "forces/s", "cores": sm["threads"],
                              "kind": "port",
-                             "sample": f"per step: full tree build + walk of {samples} seeded targets, "
-                                       "scaled to N (the Fortran reference cannot be compiled here: "
-                                       "no Fortran compiler)"},
+                             "sample": f"per step: one full force evaluation of N={n} (serial tree "
+                                       f"build + OpenMP walk of all N targets); the Fortran "
+                                       f"reference cannot be compiled here: no Fortran compiler",
+                             "build_s": sm["median_build_s"], "walk_s": sm["median_walk_s"],
+                             "per_step_s": sm["per_run_s"]},
             "e2e": {"value": value, "unit": "forces/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -798,7 +852,8 @@ def run_serving_sweep(args):
         met = run(requests(), rate=load * cap_rps)
         rates.append({"load": load, "rate_rps": load * cap_rps, "p50_ms": met["p50_ms"],
                       "p99_ms": met["p99_ms"], "forces_per_s": met["forces_per_s"],
-                      "wall_s": met["wall_s"], "requests": met["requests"]})
+                      "wall_s": met["wall_s"], "requests": met["requests"],
+                      "by_kind": met["by_kind"], "paused_ticks": met["paused_ticks"]})
     sizes = [int(sp[0].numel()) for sp in specs]
     print(json.dumps({
         "metric": "serving: Poisson arrivals, rate swept (p50/p99 latency ms, forces/s)",
@@ -810,8 +865,77 @@ def run_serving_sweep(args):
                    "median_n": int(np.median(sizes)), "max_n": int(max(sizes)),
                    "force_evaluations": int(sum(sp[3] + 1 if sp[3] else 1 for sp in specs))},
         "capacity": {"requests_per_s": cap_rps, "forces_per_s": cap["forces_per_s"],
-                     "p50_ms": cap["p50_ms"], "p99_ms": cap["p99_ms"]},
+                     "p50_ms": cap["p50_ms"], "p99_ms": cap["p99_ms"], "by_kind": cap["by_kind"]},
+        "scheduling": "force requests admitted before integrations; a tick holding force "
+                      "requests takes integrations up to 2^22 bodies (at most 8 ticks out in a row)",
         "rates": rates}), flush=True)
+
+
+def run_parareal(args):
+    """The batched Parareal config: Plummer N = 16,384 (equal masses, G = 1,
+    b = 1, velocities by von Neumann sampling, seeded), velocity Verlet over
+    64 time slices of [0, 1]; coarse propagator symplectic Euler with monopole
+    theta = 0.8 forces, 2 steps per slice (dt = 1/128); fine propagator
+    velocity Verlet with quadrupole theta = 0.3, 16 steps per slice
+    (dt = 1/1024); softening 0.01; stop at the reference's error norm
+    <= 1e-20 (parareal/parareal.f90:161,174).  All slices' fine propagators
+    run as one batch per step.  Two runs: the FP32 group walk with the FP64
+    correction, and the FP64 group walk with the double-double correction.
+    For each: the error and the time of every iteration, the time to
+    convergence, the sequential fine run over the same slices and the
+    distance of the Parareal end state from it."""
+    import torch
+
+    from hierarquicos_b200 import parareal as pr
+    from hierarquicos_b200.initial_values import generate_initial_values
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, W, tf, G, eps = args.parareal_bodies, 64, 1.0, 1.0, 0.01
+    m, q, p = generate_initial_values(n, -1.0, -1.0, True, False, "plummer", (1.0, 1.0), seed=4,
+                                      velocities=True)
+    coarse = pr.Propagator("euler", "bh", 2, theta=0.8, order=1)
+    runs = []
+    for label, prec, corr in (("fp32 group walk, fp64 correction", 0, "fp64"),
+                              ("fp64 group walk, double-double correction", 1, "dd")):
+        fine = pr.Propagator("verlet", "bh", 16, theta=0.3, order=4, precision=prec)
+        # warm-up: builds the handles' workspaces
+        pr.integrate_parareal(m, q, p, tf, W, 2, 0.8, G, eps, 1e-20, 16, coarse, fine,
+                              correction=corr)
+        res = pr.integrate_parareal(m, q, p, tf, W, args.parareal_iters, 0.8, G, eps, 1e-20, 16,
+                                    coarse, fine, correction=corr)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        qs, ps = pr.sequential_fine(m, q, p, tf, W, fine, G, eps)
+        torch.cuda.synchronize()
+        seq_s = time.perf_counter() - t0
+        d = np.concatenate([(res.q[-1] - qs[-1]).ravel(), (res.p[-1] - ps[-1]).ravel()])
+
+        def time_to(tol):
+            acc = 0.0
+            for e, t in zip(res.errors, res.iteration_seconds):
+                acc += t
+                if e <= tol:
+                    return acc
+            return None
+
+        runs.append({"run": label, "correction": corr, "fine_precision": prec,
+                     "iterations": res.iterations, "converged": res.converged,
+                     "errors": res.errors, "iteration_s": res.iteration_seconds,
+                     "parareal_s": res.seconds, "sequential_fine_s": seq_s,
+                     "speedup_to_convergence": (seq_s / res.seconds) if res.converged else None,
+                     "time_to_1e-12_s": time_to(1e-12), "time_to_1e-20_s": time_to(1e-20),
+                     "end_state_vs_sequential_fine": float(np.sqrt(np.sum(d * d))) / (6 * n)})
+    print(json.dumps({
+        "metric": "batched Parareal: error per iteration (reference norm), s per iteration, "
+                  "speed-up over the sequential fine run",
+        "config": {"workload": f"plummer N={n} b=1 equal masses seeded, velocity Verlet, {W} slices "
+                               f"over [0, {tf}]", "coarse": "symplectic Euler, monopole theta 0.8, "
+                               "2 steps per slice (dt 1/128)",
+                   "fine": "velocity Verlet, quadrupole theta 0.3, 16 steps per slice (dt 1/1024)",
+                   "eps": eps, "G": G, "tolerance": 1e-20, "max_iterations": args.parareal_iters},
+        "runs": runs}), flush=True)
 
 
 def main():
@@ -820,6 +944,8 @@ def main():
         run_reference(args)
     elif args.serving_sweep:
         run_serving_sweep(args)
+    elif args.parareal:
+        run_parareal(args)
     else:
         run_ours(args)
 

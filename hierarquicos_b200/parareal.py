@@ -20,7 +20,8 @@ sweep are kept, so each iteration runs one sequential coarse sweep.  State
 and correction are FP64 on the device (the reference uses REAL(16); FP64
 limits how far below ~1e-16 relative the iterates can settle, but the
 iteration becomes exactly stationary once a window's input stops changing,
-because every propagator here is deterministic bit for bit).
+because every propagator here is deterministic bit for bit).  The correction
+can also be carried in double-double (``correction="dd"``).
 """
 from __future__ import annotations
 
@@ -80,6 +81,31 @@ class PararealResult:
     iterations: int
     seconds: float
     converged: bool
+    iteration_seconds: list = dataclasses.field(default_factory=list)
+    q_lo: np.ndarray | None = None  # correction "dd": low parts of the state (q + q_lo)
+    p_lo: np.ndarray | None = None
+
+
+def _two_sum(a: torch.Tensor, b: torch.Tensor):
+    """s + e = a + b exactly, s = fl(a + b) (Knuth's TwoSum; every torch
+    elementwise operation here is one separately rounded FP64 operation)."""
+    s = a + b
+    bb = s - a
+    e = (a - (s - bb)) + (b - bb)
+    return s, e
+
+
+def _dd_correction(g: torch.Tensor, f: torch.Tensor, g_old: torch.Tensor):
+    """(G(U_{k+1}) + F(U_k)) - G(U_k) of parareal.f90:153-156 in double-double:
+    the three FP64 terms are added with TwoSum and the result is returned as
+    a normalised pair (hi, lo) with hi + lo within 2^-104 relative of the exact
+    sum (hi is the exact sum rounded to FP64 up to one ulp)."""
+    s, e1 = _two_sum(g, f)
+    t, e2 = _two_sum(s, -g_old)
+    lo = e1 + e2
+    hi = t + lo
+    lo = lo - (hi - t)
+    return hi, lo
 
 
 def _window(st: BatchState, i: int, n: int):
@@ -89,9 +115,21 @@ def _window(st: BatchState, i: int, n: int):
 def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, theta: float,
                        G: float, eps: float, maxerror: float, qntt: int,
                        coarse: Propagator | None = None, fine: Propagator | None = None,
-                       verbose: bool = False, device=None) -> PararealResult:
+                       verbose: bool = False, device=None,
+                       correction: str = "fp64") -> PararealResult:
     """Parareal with the reference's arguments (parareal/parareal.f90:97);
-    ``coarse``/``fine`` default to the reference's G_til / F_til."""
+    ``coarse``/``fine`` default to the reference's G_til / F_til.
+
+    ``correction`` "fp64" evaluates the update (G_new + F) - G_old in FP64 as
+    the source text reads; "dd" evaluates it exactly (double-double, see
+    _dd_correction) and keeps each window's state as an FP64 pair hi + lo: the
+    propagators start from hi, the error norm is taken on hi + lo, and the
+    low parts are returned in q_lo / p_lo.  The reference works in REAL(16)
+    (113-bit significand); the pair carries 106 bits of the state between
+    iterations while the propagators themselves stay FP64."""
+    if correction not in ("fp64", "dd"):
+        raise ValueError("correction must be 'fp64' or 'dd'")
+    dd = correction == "dd"
     coarse = coarse or reference_coarse(theta)
     fine = fine or reference_fine(qntt)
     dev = as_device(device)
@@ -128,12 +166,17 @@ def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, t
 
     fin_offs = np.arange(W, dtype=np.int64) * n
     mW1 = U.m[:(W - 1) * n]
+    q_lo = torch.zeros_like(U.q)  # low parts of the state (correction "dd")
+    p_lo = torch.zeros_like(U.p)
     errors = []
+    it_seconds = []
     iterations = 1
+    torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     converged = False
     for _ in range(n_itermax - 1):
         iterations += 1
+        t_it = time.perf_counter()
         # fine propagators of windows 0..W-2, one batch
         Fst = BatchState(mW1, U.q[:, :(W - 1) * n].contiguous(),
                          U.p[:, :(W - 1) * n].contiguous(), fin_offs, dev)
@@ -141,6 +184,8 @@ def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, t
         # sequential correction
         Uq = U.q.clone()
         Up = U.p.clone()
+        Uq_lo = q_lo.clone()
+        Up_lo = p_lo.clone()
         Gq_new = torch.empty_like(Gq_old)
         Gp_new = torch.empty_like(Gp_old)
         for i in range(W - 1):
@@ -149,16 +194,29 @@ def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, t
             Gq_new[:, w] = gq
             Gp_new[:, w] = gp
             w1 = _window(U, i + 1, n)
-            Uq[:, w1] = (gq + Fst.q[:, w]) - Gq_old[:, w]
-            Up[:, w1] = (gp + Fst.p[:, w]) - Gp_old[:, w]
+            if dd:
+                Uq[:, w1], Uq_lo[:, w1] = _dd_correction(gq, Fst.q[:, w], Gq_old[:, w])
+                Up[:, w1], Up_lo[:, w1] = _dd_correction(gp, Fst.p[:, w], Gp_old[:, w])
+            else:
+                Uq[:, w1] = (gq + Fst.q[:, w]) - Gq_old[:, w]
+                Up[:, w1] = (gp + Fst.p[:, w]) - Gp_old[:, w]
         last = _window(U, W - 1, n)
-        d = torch.cat([(Uq[:, last] - U.q[:, last]).reshape(-1),
-                       (Up[:, last] - U.p[:, last]).reshape(-1)])
+        if dd:
+            # (hi + lo) - (hi' + lo'): the hi difference is exact for close
+            # values (Sterbenz), the lo difference is far below it
+            dq = (Uq[:, last] - U.q[:, last]) + (Uq_lo[:, last] - q_lo[:, last])
+            dp = (Up[:, last] - U.p[:, last]) + (Up_lo[:, last] - p_lo[:, last])
+        else:
+            dq = Uq[:, last] - U.q[:, last]
+            dp = Up[:, last] - U.p[:, last]
+        d = torch.cat([dq.reshape(-1), dp.reshape(-1)])
         err = float(torch.sqrt(torch.sum(d * d))) / (6 * n)
         errors.append(err)
         U.q.copy_(Uq)
         U.p.copy_(Up)
+        q_lo, p_lo = Uq_lo, Up_lo
         Gq_old, Gp_old = Gq_new, Gp_new
+        it_seconds.append(time.perf_counter() - t_it)  # float() above synchronised
         if verbose:
             print(f"Iter.: {iterations:4d} / Error: {err:12.4e}", flush=True)
         if err <= maxerror:
@@ -168,7 +226,11 @@ def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, t
     seconds = time.perf_counter() - t0
     q = U.q.T.reshape(W, n, 3).cpu().numpy()
     p = U.p.T.reshape(W, n, 3).cpu().numpy()
-    return PararealResult(q, p, errors, iterations, seconds, converged)
+    res = PararealResult(q, p, errors, iterations, seconds, converged, it_seconds)
+    if dd:
+        res.q_lo = q_lo.T.reshape(W, n, 3).cpu().numpy()
+        res.p_lo = p_lo.T.reshape(W, n, 3).cpu().numpy()
+    return res
 
 
 def sequential_fine(m, q0, p0, tf: float, num_windows: int, fine: Propagator, G: float,

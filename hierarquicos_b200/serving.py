@@ -84,6 +84,9 @@ class Request:
             raise ValueError("a leapfrog request needs momenta and steps >= 1")
         self._done = threading.Event()
         self._evals = 0  # force evaluations done
+        self._last_tick = -1  # last tick of its lane that evaluated it
+        self._paused = 0      # ticks sat out in a row
+        self._passed = 0      # admission rounds in which a later request went first
 
     @property
     def evals_needed(self) -> int:
@@ -136,6 +139,7 @@ class _Lane:
         self.done_cv = threading.Condition()
         self.ticks = 0
         self.tick_bodies = 0
+        self.paused_ticks = 0              # integrations that sat a tick out
         # per tick: host seconds spent enqueuing it and CUDA events around its
         # device work (read by Server.metrics)
         self.tick_log: collections.deque = collections.deque(maxlen=4096)
@@ -149,14 +153,38 @@ class _Lane:
         self.buf = []
         self.out = self.d_off = self.d_coef = None
 
-    # -- one tick: forces of every active system, then the per-system kicks --
+    def _schedule(self, act: list[Request]) -> tuple[list[Request], list[Request]]:
+        """Which of the lane's systems this tick evaluates.  Without force
+        requests in the lane every system runs.  With some, the force requests
+        run and integrations join them only while the tick stays within the
+        server's ``force_tick_bodies`` (least recently run first); the others
+        sit this tick out, their state carried over unchanged.  An integration
+        that has sat out ``max_pause_ticks`` ticks in a row runs regardless,
+        so a stream of force requests cannot stall it."""
+        srv = self.server
+        forces = [r for r in act if r.kind == "force"]
+        if not forces or srv.force_tick_bodies is None:
+            return act, []
+        budget = srv.force_tick_bodies - sum(r.n for r in forces)
+        run, paused = list(forces), []
+        for r in sorted((r for r in act if r.kind == "leapfrog"), key=lambda r: r._last_tick):
+            if r.n <= budget or r._paused >= srv.max_pause_ticks:
+                run.append(r)
+                budget -= r.n
+            else:
+                paused.append(r)
+        return run, paused
+
+    # -- one tick: forces of every running system, then the per-system kicks --
     def _tick(self):
         srv = self.server
-        act = self.active + self.fresh
+        run, paused = self._schedule(self.active + self.fresh)
+        act = run + paused  # running systems first: the tick evaluates [0, n)
+        nrun = len(run)
         sizes = [r.n for r in act]
         off = np.zeros(len(act) + 1, np.int64)
         off[1:] = np.cumsum(sizes)
-        n = int(off[-1])
+        n = int(off[nrun])
         src, dst = self.buf[self.cur], self.buf[1 - self.cur]
         t_host = time.perf_counter()
         ev_begin = torch.cuda.Event(enable_timing=True)
@@ -191,12 +219,11 @@ class _Lane:
             if host_new:
                 self.stream.wait_event(ev_in)
             out = self.out[:3 * n]
-            self.sys.forces_batch(dst[0, :n], dst[1, :n], dst[2, :n], dst[3, :n], off, srv.params,
-                                  out=out)
-            leap = [r.kind == "leapfrog" for r in act]
-            if any(leap):
+            self.sys.forces_batch(dst[0, :n], dst[1, :n], dst[2, :n], dst[3, :n], off[:nrun + 1],
+                                  srv.params, out=out)
+            if any(r.kind == "leapfrog" for r in run):
                 coef = self.h_coef.numpy()
-                for i, r in enumerate(act):
+                for i, r in enumerate(run):
                     c = (0.0, 0.0, 0.0)
                     if r.kind == "leapfrog":
                         h = 0.5 * r.dt
@@ -204,20 +231,24 @@ class _Lane:
                         c = (0.0, h, r.dt) if k == 0 else ((h, h, r.dt) if k < r.steps
                                                            else (h, 0.0, 0.0))
                     coef[3 * i:3 * i + 3] = c
-                self.h_off.numpy()[:len(act) + 1] = off
-                self.d_coef[:3 * len(act)].copy_(self.h_coef[:3 * len(act)], non_blocking=True)
-                self.d_off[:len(act) + 1].copy_(self.h_off[:len(act) + 1], non_blocking=True)
+                self.h_off.numpy()[:nrun + 1] = off[:nrun + 1]
+                self.d_coef[:3 * nrun].copy_(self.h_coef[:3 * nrun], non_blocking=True)
+                self.d_off[:nrun + 1].copy_(self.h_off[:nrun + 1], non_blocking=True)
                 check(lib().bh_kick_drift_systems(
                     _dptr(dst[0]), _dptr(out), _dptr(dst[1]), _dptr(dst[2]), _dptr(dst[3]),
-                    _dptr(dst[4]), _dptr(dst[5]), _dptr(dst[6]), _dptr(self.d_off), len(act), n,
+                    _dptr(dst[4]), _dptr(dst[5]), _dptr(dst[6]), _dptr(self.d_off), nrun, n,
                     _dptr(self.d_coef), self.stream.cuda_stream))
-            for r in act:
+            for r in run:
                 r._evals += 1
+                r._last_tick = self.ticks
+                r._paused = 0
+            for r in paused:
+                r._paused += 1
             # device results: copied into the request's own buffers
             finished, keep = [], []
             for i, r in enumerate(act):
                 a, b = int(off[i]), int(off[i + 1])
-                if r._evals >= r.evals_needed:
+                if i < nrun and r._evals >= r.evals_needed:
                     finished.append((r, a, b))
                     if r.on_device:
                         if r.kind == "force":
@@ -256,6 +287,7 @@ class _Lane:
         self.fresh = []
         self.ticks += 1
         self.tick_bodies += n
+        self.paused_ticks += len(paused)
 
     def _run(self):
         srv = self.server
@@ -322,12 +354,24 @@ class Server:
     ``params``: engine parameters (theta, eps, order, ...; default theta 0.5,
     quadrupole).  ``hbm_budget``: bytes the server may hold on the device.
     ``max_tick_bodies``: bodies of one lane's tick (bounds the lanes'
-    workspaces and a tick's latency)."""
+    workspaces and a tick's latency).  ``force_tick_bodies``: while a lane
+    holds force requests its ticks take integrations only up to this many
+    bodies in all (the rest sit the tick out, at most ``max_pause_ticks`` in a
+    row).  Admission takes force requests before integrations, FIFO within
+    each kind, and lets a later request that fits go ahead of one that does
+    not, until the one passed over has waited ``max_passed`` rounds."""
 
     def __init__(self, params: BHParams | None = None, device=None, hbm_budget: float = 150e9,
                  max_tick_bodies: int = 1 << 23, lanes: int = 2, max_tick_systems: int = 4096,
-                 **kw):
+                 force_tick_bodies: int | None = 1 << 22, max_pause_ticks: int = 8,
+                 max_passed: int = 64, **kw):
         self.device = as_device(device)
+        # scheduling: force requests are admitted ahead of integrations, and a
+        # tick that holds force requests takes integrations only up to
+        # force_tick_bodies bodies (None: every active system runs every tick)
+        self.force_tick_bodies = None if force_tick_bodies is None else int(force_tick_bodies)
+        self.max_pause_ticks = int(max_pause_ticks)
+        self.max_passed = int(max_passed)
         self.params = params if params is not None else default_params(**kw)
         self.hbm_budget = float(hbm_budget)
         self.max_tick_bodies = int(max_tick_bodies)
@@ -487,27 +531,39 @@ class Server:
         return not self._pending
 
     def _admit(self, lane: _Lane) -> list[Request]:
-        """FIFO admission of pending requests into this lane while they fit the
-        HBM budget and the lane's tick capacity."""
+        """Admission of pending requests into this lane while they fit the HBM
+        budget and the lane's tick capacity: force requests first, then
+        integrations, FIFO within each kind.  A request that does not fit is
+        passed over for later ones that do; once it has been passed over
+        ``max_passed`` times nothing behind it is admitted until it fits."""
         out = []
         with self._cv:
             room = self.hbm_budget - self.workspace_bytes
             bodies = sum(r.n for r in lane.active)
             systems = len(lane.active)
-            while self._pending:
-                r = self._pending[0]
+            order = sorted(range(len(self._pending)),
+                           key=lambda i: (self._pending[i].kind != "force", i))
+            taken = set()
+            for i in order:
+                r = self._pending[i]
                 fp = self.footprint(r.n)
                 if (self._resident + fp > room or bodies + r.n > self.max_tick_bodies
                         or systems + 1 > self.max_tick_systems):
-                    break
+                    r._passed += 1
+                    if r._passed > self.max_passed:
+                        break
+                    continue
                 systems += 1
-                self._pending.popleft()
+                taken.add(i)
                 self._resident += fp
                 self.max_resident = max(self.max_resident, self._resident)
                 bodies += r.n
                 r.t_admit = time.perf_counter()
                 r.lane = lane.index
                 out.append(r)
+            if taken:
+                self._pending = collections.deque(
+                    r for i, r in enumerate(self._pending) if i not in taken)
         return out
 
     def _release(self, r: Request):
@@ -543,8 +599,16 @@ class Server:
                  "device_ms_max": float(np.max(dev_ms)) if dev_ms else None,
                  "lane_gap_ms_mean": float(np.mean(gap_ms)) if gap_ms else None,
                  "lane_gap_ms_max": float(np.max(gap_ms)) if gap_ms else None}
+        by_kind = {}
+        for kind in ("force", "leapfrog"):
+            lk = np.array([r.latency for r in rs if r.kind == kind]) * 1e3
+            if lk.size:
+                by_kind[kind] = {"requests": int(lk.size), "p50_ms": float(np.percentile(lk, 50)),
+                                 "p99_ms": float(np.percentile(lk, 99))}
         return {"requests": len(rs), "p50_ms": float(np.percentile(lat, 50)),
                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "by_kind": by_kind,
+                "paused_ticks": sum(ln.paused_ticks for ln in self.lanes),
                 "wall_s": t1 - t0, "forces": int(forces), "forces_per_s": forces / (t1 - t0),
                 "ticks": sum(ln.ticks for ln in self.lanes),
                 "mean_tick_bodies": sum(ln.tick_bodies for ln in self.lanes)

@@ -114,6 +114,10 @@ def test_dehnen_batch_equals_single_systems(bh):
         fs = single.forces(ms[k], *xyz(qs[k]), **kw).cpu().numpy()
         assert np.array_equal(f[3 * a:3 * b], fs), f"system {k} (n={n})"
     assert np.all(f[0:3] == 0.0)  # a lone body feels nothing
+    # the traversal's lists have one order whatever the schedule: run to run
+    # the bits do not change
+    f2 = s.forces_batch(m, *xyz(q), off, **kw).cpu().numpy()
+    assert np.array_equal(f, f2)
 
 
 def test_dehnen_two_bodies_is_exact(bh):

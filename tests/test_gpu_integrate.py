@@ -175,3 +175,61 @@ def test_parareal_becomes_stationary_at_the_fine_solution(ig):
     qs, ps = pr.sequential_fine(m, q, p, tf, W, fine, G, eps)
     np.testing.assert_allclose(res.q, qs, rtol=1e-12, atol=1e-13)
     np.testing.assert_allclose(res.p, ps, rtol=1e-9, atol=1e-15)
+
+
+def test_parareal_double_double_correction(ig, oracle_mod):
+    """The double-double correction: hi + lo is the exact value of
+    (G_new + F) - G_old, so hi is the FP64 correction rounded once (it may
+    differ from the twice-rounded FP64 form by an ulp) and |lo| is at most half
+    an ulp of hi; the error curve is that of the FP64 correction."""
+    from hierarquicos_b200 import parareal as pr
+
+    m, q, p = plummer_state(64, seed=9)
+    G, eps, tf, W, itmax = 1.0, 0.05, 0.4, 6, 5
+    coarse = pr.Propagator("euler", "direct", 1)
+    fine = pr.Propagator("verlet", "direct", 8)
+    a = pr.integrate_parareal(m, q, p, tf, W, itmax, 0.5, G, eps, 0.0, 8, coarse, fine)
+    b = pr.integrate_parareal(m, q, p, tf, W, itmax, 0.5, G, eps, 0.0, 8, coarse, fine,
+                              correction="dd")
+    assert b.q_lo is not None and b.iterations == a.iterations
+    np.testing.assert_allclose(b.q, a.q, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(b.p, a.p, rtol=1e-10, atol=1e-15)
+    assert np.all(np.abs(b.q_lo) <= 0.5 * np.spacing(np.abs(b.q)))
+    assert np.all(np.abs(b.p_lo) <= 0.5 * np.spacing(np.abs(b.p)))
+    assert np.any(b.q_lo != 0.0)
+    big = [k for k, e in enumerate(a.errors) if e > 1e-13]
+    np.testing.assert_allclose(np.array(b.errors)[big], np.array(a.errors)[big], rtol=1e-5)
+
+
+def test_parareal_reference_example_config(ig, oracle_mod):
+    """The configuration of parareal/main.f90 (N = 1000 in the cube [-10, 10]^3,
+    m = 1/N, p = 0, G = 1, eps = 0.5, tf = 10, 30 windows, 16 fine Verlet steps
+    per window, direct forces in both propagators -- its "PARAREAL (direct)"
+    run) on seeded positions: the device's error curve equals the restated
+    integrate_parareal's and falls geometrically until the FP64 floor."""
+    from hierarquicos_b200 import parareal as pr
+    from oracle import integrate as oi
+
+    N, G, eps, tf, W, qntt, itmax = 1000, 1.0, 0.5, 10.0, 30, 16, 5
+    rng = np.random.Generator(np.random.PCG64(0))
+    m = np.full(N, 1.0 / N)
+    q = 10.0 * (2.0 * rng.random((N, 3)) - 1.0)
+    p = np.zeros((N, 3))
+    coarse = pr.Propagator("euler", "direct", 1)
+    fine = pr.Propagator("verlet", "direct", qntt)
+    res = pr.integrate_parareal(m, q, p, tf, W, itmax, -1.0, G, eps, 1e-20, qntt, coarse, fine)
+
+    def forces(mm, qq):
+        return oracle_mod.direct_forces(mm, qq[:, 0], qq[:, 1], qq[:, 2], G, eps * eps)
+
+    window = tf / W
+    _, errs, its = oi.parareal(
+        m, q, p, tf, W, itmax, 1e-20,
+        lambda mm, qq, pp: oi.symplectic_euler(mm, qq, pp, window, 1, forces),
+        lambda mm, qq, pp: oi.verlet(mm, qq, pp, window / qntt, qntt, forces))
+    assert res.iterations == its
+    big = [k for k, e in enumerate(errs) if e > 1e-12]
+    assert len(big) >= 3
+    np.testing.assert_allclose(np.array(res.errors)[big], np.array(errs)[big], rtol=1e-5)
+    e = np.array(res.errors)
+    assert np.all(e[1:len(big)] < 1e-2 * e[:len(big) - 1])  # each iteration gains > 2 decades

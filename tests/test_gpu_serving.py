@@ -194,3 +194,21 @@ def test_submit_many_queues_a_group_at_once(sv):
     with pytest.raises(ValueError):
         srv.submit_many([small, sv.Request("force", m, q)])
     assert len(srv._pending) == 0
+
+
+def test_paused_integrations_match_plain_path(sv):
+    """With a small force_tick_bodies the lanes make integrations sit ticks
+    out while force requests run (and force requests are admitted first); the
+    results are still exactly the plain path's, and some ticks did pause."""
+    reqs = mixed_requests(sv, 16, seed=5)
+    with sv.Server(hbm_budget=40e9, max_tick_bodies=1 << 20, force_tick_bodies=3000,
+                   max_pause_ticks=2, **PARAMS) as srv:
+        srv.submit_many(reqs)
+        srv.drain(timeout=300)
+        met = srv.metrics()
+    assert met["requests"] == len(reqs)
+    assert met["paused_ticks"] > 0
+    assert set(met["by_kind"]) <= {"force", "leapfrog"}
+    for r in reqs:
+        assert r.error is None
+        check_against_plain(r)

@@ -134,3 +134,70 @@ def test_sharded_outputs_combine_to_the_full_result(world):
         p.join(timeout=60)
         assert p.exitcode == 0
     assert all(res.values()), res
+
+
+def test_rebalance_moves_cut_points_toward_equal_cost():
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from hierarquicos_b200.shard import rebalance
+
+    rng = np.random.default_rng(3)
+    n_groups, world = 16384, 4
+    # group cost rises toward the middle (a centrally concentrated system)
+    cost = 1.0 + 5.0 * np.exp(-((np.arange(n_groups) - n_groups / 2) / 1500.0) ** 2)
+    cost *= rng.uniform(0.8, 1.2, n_groups)
+    bounds = [0, 4096, 8192, 12288, 16384]
+
+    def times(b):
+        return [cost[b[r]:b[r + 1]].sum() for r in range(world)]
+
+    imb0 = max(times(bounds)) / np.mean(times(bounds))
+    for _ in range(6):
+        bounds = rebalance(bounds, times(bounds))
+        assert bounds[0] == 0 and bounds[-1] == n_groups
+        assert all(bounds[i] <= bounds[i + 1] for i in range(world))
+    imb = max(times(bounds)) / np.mean(times(bounds))
+    assert imb0 > 1.3 and imb < 1.03, (imb0, imb)
+    # equal times keep the cut points
+    assert rebalance([0, 10, 20, 30], [1.0, 1.0, 1.0]) == [0, 10, 20, 30]
+    # empty ranges are allowed and stay ordered
+    b = rebalance([0, 0, 50, 100], [0.0, 3.0, 1.0])
+    assert b[0] == 0 and b[-1] == 100 and b == sorted(b)
+
+
+def _balance_worker(rank, world, port, q):
+    """Every rank reports its own time; all ranks must agree on the new cut
+    points."""
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, ROOT)
+    from hierarquicos_b200.shard import Balancer
+
+    bal = Balancer(world)
+    bal.range(1000, rank)
+    got = bal.update(10.0 * (rank + 1))
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, (got, bal.bounds)))
+
+
+def test_balancer_agrees_on_all_ranks():
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_balance_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res[0] == res[1]
+    times, bounds = res[0]
+    assert times == [10.0, 20.0]
+    assert bounds[0] == 0 and bounds[-1] == 1000 and bounds[1] > 500  # rank 1 was slower
