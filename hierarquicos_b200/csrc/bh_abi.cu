@@ -46,6 +46,11 @@ struct bh_system {
   bool layout_pending = false;
   // Dehnen's method, allocated on first use
   bh::DehnenBuffers dehnen;
+  // host-array entry points: the four input copies run on four streams at
+  // once (one copy engine stream does not fill the host link), created on
+  // first use
+  cudaStream_t copy_st[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t copy_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -468,10 +473,25 @@ int stage_inputs(bh_system *s, const double *m, const double *x, const double *y
   rc = ensure_host_staging(s, n);
   if (rc) return rc;
   Buffers &b = s->b;
+  if (!s->copy_ev[0]) {
+    for (int k = 0; k < 3; ++k)
+      BH_CUDA(cudaStreamCreateWithFlags(&s->copy_st[k], cudaStreamNonBlocking));
+    for (int k = 0; k < 4; ++k)
+      BH_CUDA(cudaEventCreateWithFlags(&s->copy_ev[k], cudaEventDisableTiming));
+  }
+  // the copy streams start after the work already queued on st (the staging
+  // buffers may still be read by it); st then waits for all four copies
+  BH_CUDA(cudaEventRecord(s->copy_ev[3], st));
+  const double *src[3] = {x, y, z};
+  double *dst[3] = {b.hx, b.hy, b.hz};
+  for (int k = 0; k < 3; ++k) {
+    BH_CUDA(cudaStreamWaitEvent(s->copy_st[k], s->copy_ev[3], 0));
+    BH_CUDA(cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice,
+                            s->copy_st[k]));
+    BH_CUDA(cudaEventRecord(s->copy_ev[k], s->copy_st[k]));
+  }
   BH_CUDA(cudaMemcpyAsync(b.hm, m, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hx, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));
-  BH_CUDA(cudaMemcpyAsync(b.hz, z, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < 3; ++k) BH_CUDA(cudaStreamWaitEvent(st, s->copy_ev[k], 0));
   return BH_OK;
 }
 
@@ -550,6 +570,10 @@ int bh_system_destroy(bh_system *s) {
   if (!s->fixed_buffers) free_buffers(s->b);
   if (s->items_pin) cudaFreeHost(s->items_pin);
   if (s->layout_ev) cudaEventDestroy(s->layout_ev);
+  for (int k = 0; k < 3; ++k)
+    if (s->copy_st[k]) cudaStreamDestroy(s->copy_st[k]);
+  for (int k = 0; k < 4; ++k)
+    if (s->copy_ev[k]) cudaEventDestroy(s->copy_ev[k]);
   delete s;
   return BH_OK;
 }

@@ -133,8 +133,8 @@ def test_2_21_system_inside_a_batch(bh, oracle_mod):
     local[sel] = np.arange(sel.size)
     lm = meta[sel].astype(np.int64)
     lm[:, 0] -= a
-    lc = child[sel].astype(np.int64)
     used = np.arange(8)[None, :] < lm[:, 3:4]
+    lc = np.where(used, child[sel].astype(np.int64), 0)  # entries past nchild are unset
     lc = np.where(lc >= 0, local[np.maximum(lc, 0)], ~(~lc - a))
     lc = np.where(used, lc, 0)
     ref = oracle_mod.MortonTree(m1, *xyz(q1), L=21, use_quadrupole=False, fma_mode=1)
