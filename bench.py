@@ -118,7 +118,7 @@ def parse():
                     help="instead of the headline line: the batched Parareal config (Plummer "
                          "16384, 64 slices, coarse monopole theta 0.8, fine quadrupole theta 0.3)")
     ap.add_argument("--parareal-bodies", type=int, default=16384)
-    ap.add_argument("--parareal-iters", type=int, default=24)
+    ap.add_argument("--parareal-iters", type=int, default=40)
     ap.add_argument("--no-extras", action="store_true",
                     help="plain timed calls only (no serving, error check, e2e, batch or CPU baseline)")
     return ap.parse_args()
