@@ -138,7 +138,9 @@ __global__ void roots_frontier_kernel(const SysScalars *__restrict__ ss, int nsy
   if (s == 0) *nout = (unsigned long long)nsys;
 }
 
-constexpr int kGenThreads = 256;            // one input pair per thread, one tile per block
+constexpr int kGenThreads = 256;            // threads of a block; one tile per block at a time
+constexpr int kGenItems = 4;                // consecutive input pairs per thread
+constexpr int kGenTile = kGenThreads * kGenItems;
 constexpr int kGenWarps = kGenThreads / kWarp;
 // tile words of the chained scan: top 2 bits the state, low 62 bits the count
 constexpr uint64_t kGenAggregate = 1ull << 62;  // the tile's own count
@@ -209,16 +211,64 @@ __device__ __forceinline__ int64_t gen_lookback(uint64_t *status, int t, int64_t
   return excl;
 }
 
+// Classification of one input pair (a, b): kind 0 nothing, 1 the children
+// pairs of a self pair, 2 a mutual interaction, 3 open member `o` against
+// `other`; n_out new frontier pairs.
+struct GenPair {
+  int kind, k;
+  int64_t a, b, o, other;
+  bool open_a;
+  int4 mt;
+};
+
+__device__ __forceinline__ GenPair classify_pair(const Ent &e, int2 ab, double theta2,
+                                                 unsigned long long *flags) {
+  GenPair g;
+  g.kind = 0; g.k = 0; g.a = ab.x; g.b = ab.y; g.o = 0; g.other = 0; g.open_a = false;
+  g.mt = make_int4(0, 0, 0, 0);
+  if (g.a < 0 || g.b < 0) return g;
+  const double4 ca = ent_com(e, g.a), cb = ent_com(e, g.b);
+  if (ca.w == 0.0 || cb.w == 0.0) return g;
+  if (g.a == g.b) {
+    if (g.a < e.n) {  // a body with itself is dropped
+      g.mt = e.meta[g.a];
+      g.k = node_nchild(g.mt);
+      g.kind = 1;
+    }
+    return g;
+  }
+  const double dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
+  const double dist2 = dx * dx + dy * dy + dz * dz;
+  const double ra = ent_rmax(e, g.a), rb = ent_rmax(e, g.b);
+  const double rs = ra + rb;
+  if (rs * rs <= theta2 * dist2) {
+    g.kind = 2;
+    return g;
+  }
+  g.open_a = ra >= rb;
+  g.o = g.open_a ? g.a : g.b;
+  g.other = g.open_a ? g.b : g.a;
+  if (g.o >= e.n) {
+    atomicOr(flags, 4ull);  // cannot happen: bodies have rmax 0
+    return g;
+  }
+  g.mt = e.meta[g.o];
+  g.k = node_nchild(g.mt);
+  g.kind = 3;
+  return g;
+}
+
 // One generation of the dual traversal, as a deterministic compaction: block
-// tiles of kGenThreads input pairs are claimed in order from `tile_ctr`; every
-// thread classifies its pair, the block scans the counts of new frontier
-// pairs and of mutual pairs, and a chained scan over the tiles (separate
-// status words for the two lists) places every pair's outputs right after
-// those of the pairs before it.  So both lists come out in input order,
-// whatever the schedule: the frontier of the next generation, and the mutual
-// pairs appended after the `mut_base` written by earlier generations.  The
-// block of the last tile writes the two new totals (the next generation's
-// input count and the mutual count after this generation).
+// tiles of kGenTile input pairs (kGenItems consecutive pairs per thread) are
+// claimed in order from `tile_ctr`; every thread classifies its pairs, the
+// block scans the counts of new frontier pairs and of mutual pairs, and a
+// chained scan over the tiles (separate status words for the two lists)
+// places every pair's outputs right after those of the pairs before it.  So
+// both lists come out in input order, whatever the schedule: the frontier of
+// the next generation, and the mutual pairs appended after the `mut_base`
+// written by earlier generations.  The block of the last tile writes the two
+// new totals (the next generation's input count and the mutual count after
+// this generation).
 __global__ void __launch_bounds__(kGenThreads)
 dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *__restrict__ nin,
                 int64_t cap_in, int2 *__restrict__ fout, unsigned long long *nout, int64_t cap_out,
@@ -232,7 +282,7 @@ dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *_
   // after an overflow the count exceeds what was written: read only the buffer
   const int64_t n_in = bh_min64((int64_t)*nin, cap_in);
   const int64_t mut_base = (int64_t)*nmut_in;
-  const int64_t ntiles = (n_in + kGenThreads - 1) / kGenThreads;
+  const int64_t ntiles = (n_in + kGenTile - 1) / kGenTile;
   if (ntiles == 0) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { *nout = 0; *nmut_out = (unsigned long long)mut_base; }
     return;
@@ -243,48 +293,20 @@ dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *_
     const int t = s_tile;
     __syncthreads();
     if ((int64_t)t >= ntiles) break;  // uniform across the block
-    const int64_t i = (int64_t)t * kGenThreads + threadIdx.x;
-    // kind: 0 nothing, 1 children pairs of a self pair, 2 mutual, 3 open `o`
-    int kind = 0, k = 0;
-    int64_t a = -1, b = -1, o = 0, other = 0;
-    bool open_a = false;
-    int4 mt = make_int4(0, 0, 0, 0);
-    if (i < n_in) {
-      a = fin[i].x; b = fin[i].y;
+    const int64_t i0 = (int64_t)t * kGenTile + (int64_t)threadIdx.x * kGenItems;
+    int2 ab[kGenItems];
+#pragma unroll
+    for (int q = 0; q < kGenItems; ++q) ab[q] = i0 + q < n_in ? fin[i0 + q] : make_int2(-1, -1);
+    GenPair g[kGenItems];
+#pragma unroll
+    for (int q = 0; q < kGenItems; ++q) g[q] = classify_pair(e, ab[q], theta2, flags);
+    // this thread's outputs, in input order
+    int n_out = 0, n_mut = 0;
+#pragma unroll
+    for (int q = 0; q < kGenItems; ++q) {
+      n_out += g[q].kind == 1 ? g[q].k * (g[q].k + 1) / 2 : (g[q].kind == 3 ? g[q].k : 0);
+      n_mut += g[q].kind == 2 ? 1 : 0;
     }
-    if (a >= 0 && b >= 0) {
-      const double4 ca = ent_com(e, a), cb = ent_com(e, b);
-      if (ca.w != 0.0 && cb.w != 0.0) {
-        if (a == b) {
-          if (a < e.n) {  // a body with itself is dropped
-            mt = e.meta[a];
-            k = node_nchild(mt);
-            kind = 1;
-          }
-        } else {
-          const double dx = ca.x - cb.x, dy = ca.y - cb.y, dz = ca.z - cb.z;
-          const double dist2 = dx * dx + dy * dy + dz * dz;
-          const double ra = ent_rmax(e, a), rb = ent_rmax(e, b);
-          const double rs = ra + rb;
-          if (rs * rs <= theta2 * dist2) {
-            kind = 2;
-          } else {
-            open_a = ra >= rb;
-            o = open_a ? a : b;
-            other = open_a ? b : a;
-            if (o >= e.n) {
-              atomicOr(flags, 4ull);  // cannot happen: bodies have rmax 0
-            } else {
-              mt = e.meta[o];
-              k = node_nchild(mt);
-              kind = 3;
-            }
-          }
-        }
-      }
-    }
-    const int n_out = kind == 1 ? k * (k + 1) / 2 : (kind == 3 ? k : 0);
-    const int n_mut = kind == 2 ? 1 : 0;
     int tot_f, tot_m;
     const int off_f = gen_block_scan(n_out, ws, &tot_f);
     const int off_m = gen_block_scan(n_mut, ws, &tot_m);
@@ -299,21 +321,33 @@ dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *_
       }
     }
     __syncthreads();
-    const int64_t fo = s_base[0] + off_f, mo = s_base[1] + off_m;
+    int64_t fo = s_base[0] + off_f, mo = s_base[1] + off_m;
     if (n_out > 0 && fo + n_out > cap_out) atomicOr(flags, 1ull);
     if (n_mut > 0 && mo + n_mut > cap_mut) atomicOr(flags, 2ull);
-    if (kind == 2 && mo < cap_mut) mut[mo] = make_int2((int)a, (int)b);
-    if (kind == 1 && fo + n_out <= cap_out) {
-      int64_t w = fo;
-      for (int p = 0; p < k; ++p) {
-        const int64_t cp = node_child(e, a, mt, p);
-        for (int q = p; q < k; ++q) fout[w++] = make_int2((int)cp, (int)node_child(e, a, mt, q));
-      }
-    }
-    if (kind == 3 && fo + n_out <= cap_out) {
-      for (int q = 0; q < k; ++q) {
-        const int64_t c = node_child(e, o, mt, q);
-        fout[fo + q] = open_a ? make_int2((int)c, (int)other) : make_int2((int)other, (int)c);
+    const bool fits_f = fo + n_out <= cap_out, fits_m = mo + n_mut <= cap_mut;
+#pragma unroll
+    for (int q = 0; q < kGenItems; ++q) {
+      const GenPair &h = g[q];
+      if (h.kind == 2) {
+        if (fits_m) mut[mo] = make_int2((int)h.a, (int)h.b);
+        ++mo;
+      } else if (h.kind == 1) {
+        if (fits_f) {
+          int64_t w = fo;
+          for (int p = 0; p < h.k; ++p) {
+            const int64_t cp = node_child(e, h.a, h.mt, p);
+            for (int r = p; r < h.k; ++r) fout[w++] = make_int2((int)cp, (int)node_child(e, h.a, h.mt, r));
+          }
+        }
+        fo += h.k * (h.k + 1) / 2;
+      } else if (h.kind == 3) {
+        if (fits_f) {
+          for (int r = 0; r < h.k; ++r) {
+            const int64_t c = node_child(e, h.o, h.mt, r);
+            fout[fo + r] = h.open_a ? make_int2((int)c, (int)h.other) : make_int2((int)h.other, (int)c);
+          }
+        }
+        fo += h.k;
       }
     }
     __syncthreads();  // s_base is rewritten by the next tile
@@ -606,7 +640,7 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
     if (grow(d.mut, d.mut_cap, d.want_mut) != cudaSuccess) return 1;
     int2 *f0 = d.front, *f1 = d.front + d.front_cap / 2;
     const int64_t fcap = d.front_cap / 2;
-    const int64_t max_tiles = fcap / kGenThreads + 1;  // tiles of one generation's input
+    const int64_t max_tiles = fcap / kGenTile + 1;  // tiles of one generation's input
     if (grow(d.gen_status, d.gen_status_cap, (int64_t)kGenerations * 2 * max_tiles) != cudaSuccess)
       return 1;
     if (grow(d.gen_tiles, d.gen_tiles_cap, (int64_t)kGenerations) != cudaSuccess) return 1;
