@@ -197,7 +197,7 @@ class ClockSampler:
 
 def launches_per_evaluation(n, nsys=1, L=21):
     """Our kernel launches in one build + walk (the pipeline's launch
-    sequence: 57 for one system of 2^20 bodies)."""
+    sequence: 54 for one system of 2^20 bodies)."""
     scan = 1                                           # one chained-scan launch
 
     def sort(bits):                                    # digit histograms, their scan, passes
@@ -212,10 +212,11 @@ def launches_per_evaluation(n, nsys=1, L=21):
     while (1 << first_bits) <= n:
         first_bits += 1
     node_sort = sort(first_bits + 5)
-    # karras, mark, scan, count, compact keys, node sort, bin2cn, records, levels, roots
-    tree = 2 + scan + 1 + 1 + node_sort + 1 + 1 + 1 + 1
+    # karras, mark, scan (also writes the node count), compact keys, node sort, bin2cn,
+    # records, levels, roots
+    tree = 2 + scan + 1 + node_sort + 1 + 1 + 1 + 1
     upward = 22                                        # one launch per level
-    groups = 1 + 1 + scan + 1 + 1                      # flags, starts, scan, count, first
+    groups = 1 + scan + 1                              # flags (and system starts), scan, first
     walk = 1
     return keys + particle_sort + by_system + 1 + tree + upward + groups + walk
 

@@ -158,9 +158,11 @@ constexpr int64_t radix_hist_entries(int64_t n) {
 }
 
 // exclusive scan of n int32 values in one launch; total written to *total
-// (device) if given; a look-back wait that gives up sets kErrTimeout in *err
+// and *total2 (device) when given; a look-back wait that gives up sets
+// kErrTimeout in *err
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
-                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s);
+                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s,
+                    int32_t *total2 = nullptr);
 
 void launch_gather(const double *m, const double *x, const double *y, const double *z, int64_t n,
                    Buffers &b, cudaStream_t s);

@@ -241,7 +241,8 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
 // tmp (int32 entries): [0] ticket, [1] unused, then one 64-bit word per tile.
 __global__ void __launch_bounds__(kScanThreads)
 scan_onepass_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n_max,
-                    const int32_t *n_dev, int32_t *tmp, int32_t *total_out, int *err) {
+                    const int32_t *n_dev, int32_t *tmp, int32_t *total_out, int32_t *total_out2,
+                    int *err) {
   __shared__ int ws[kScanThreads / kWarp];
   __shared__ int s_tile;
   __shared__ int64_t s_excl;
@@ -283,7 +284,10 @@ scan_onepass_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, i
       st_relaxed(words + t, kTileInclusive | (uint64_t)(excl + tile_total));
     }
     s_excl = excl;
-    if ((int64_t)t == ntiles - 1 && total_out) *total_out = (int32_t)(excl + tile_total);
+    if ((int64_t)t == ntiles - 1) {
+      if (total_out) *total_out = (int32_t)(excl + tile_total);
+      if (total_out2) *total_out2 = (int32_t)(excl + tile_total);
+    }
   }
   __syncthreads();
   int64_t o = s_excl + off;
@@ -336,11 +340,11 @@ static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256 && kMaxPasses
               "scan_tmp_entries / radix_hist_entries in bh_internal.cuh assume these sizes");
 
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
-                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s) {
+                    int32_t *total, int32_t *tmp, int *err, cudaStream_t s, int32_t *total2) {
   int nb = (int)((n + kScanChunk - 1) / kScanChunk);
   if (nb < 1) nb = 1;
   cudaMemsetAsync(tmp, 0, (2 + 2 * (int64_t)nb) * sizeof(int32_t), s);
-  scan_onepass_kernel<<<nb, kScanThreads, 0, s>>>(in, out, n, n_dev, tmp, total, err);
+  scan_onepass_kernel<<<nb, kScanThreads, 0, s>>>(in, out, n, n_dev, tmp, total, total2, err);
 }
 
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,

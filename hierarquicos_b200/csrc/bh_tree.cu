@@ -183,13 +183,6 @@ __global__ void roots_kernel(SysScalars *__restrict__ sys, int nsys,
   sys[s].root = sys[s].n >= 2 ? bin2cn[sys[s].off] : -1;
 }
 
-__global__ void count_to_scalars(const int32_t *__restrict__ total, Scalars *sc, int which) {
-  if (threadIdx.x == 0) {
-    if (which == 0) sc->n_compact = *total;
-    else sc->n_groups = *total;
-  }
-}
-
 // ---- target groups ----
 // Units are the subtrees of <= U bodies whose parent holds more than U bodies
 // (lone particles included).  Consecutive units under the same parent are
@@ -203,7 +196,11 @@ __global__ void count_to_scalars(const int32_t *__restrict__ total, Scalars *sc,
 __global__ void __launch_bounds__(256)
 group_flags_kernel(const int4 *__restrict__ meta, const int32_t *__restrict__ child,
                    const int32_t *__restrict__ cparent, const Scalars *__restrict__ sc, int G,
-                   int U, int32_t *__restrict__ gflag) {
+                   int U, const SysScalars *__restrict__ sys, int nsys,
+                   int32_t *__restrict__ gflag) {
+  // every system starts a group (this also covers lone bodies, which have no node)
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nsys; q += gridDim.x * blockDim.x)
+    if (sys[q].n > 0) gflag[sys[q].off] = 1;
   const int M = sc->n_compact;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
     const int4 mt = meta[j];  // first, count, level, nchild
@@ -236,13 +233,6 @@ group_flags_kernel(const int4 *__restrict__ meta, const int32_t *__restrict__ ch
   }
 }
 
-// every system starts a group (this also covers lone bodies, which have no node)
-__global__ void system_starts_kernel(const SysScalars *__restrict__ sys, int nsys,
-                                     int32_t *__restrict__ gflag) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < nsys && sys[s].n > 0) gflag[sys[s].off] = 1;
-}
-
 __global__ void __launch_bounds__(256)
 group_first_kernel(int64_t n, const int32_t *__restrict__ gflag, const int32_t *__restrict__ gscan,
                    const Scalars *__restrict__ sc, int32_t *__restrict__ g_first) {
@@ -269,8 +259,7 @@ void launch_build_tree(int64_t n, int L, Buffers &b, cudaStream_t s) {
   // rank of each marked node in binary order, total -> n_compact
   int32_t *rank = b.gscan;          // free until the group pass
   int32_t *total = b.counters + 2;  // scratch counter
-  exclusive_scan(b.bn_flag, rank, n, nullptr, total, b.scan_tmp, &b.sc->err, s);
-  count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 0);
+  exclusive_scan(b.bn_flag, rank, n, nullptr, total, b.scan_tmp, &b.sc->err, s, &b.sc->n_compact);
   // sort the compact nodes by (level, first particle)
   const int first_bits = bits_for(n);
   uint64_t *ck0 = b.k1;
@@ -294,11 +283,9 @@ void launch_groups(int64_t n, int group_size, int group_span, Buffers &b, cudaSt
   const int grid = grid_for(n, 256, 148 * 16);
   cudaMemsetAsync(b.gflag, 0, n * sizeof(int32_t), s);
   group_flags_kernel<<<grid, 256, 0, s>>>(b.cn_meta, b.cn_child, b.cn_parent, b.sc, group_size,
-                                          group_span, b.gflag);
-  system_starts_kernel<<<(b.nsys + 127) / 128, 128, 0, s>>>(b.ss, b.nsys, b.gflag);
+                                          group_span, b.ss, b.nsys, b.gflag);
   int32_t *total = b.counters + 3;
-  exclusive_scan(b.gflag, b.gscan, n, nullptr, total, b.scan_tmp, &b.sc->err, s);
-  count_to_scalars<<<1, 32, 0, s>>>(total, b.sc, 1);
+  exclusive_scan(b.gflag, b.gscan, n, nullptr, total, b.scan_tmp, &b.sc->err, s, &b.sc->n_groups);
   group_first_kernel<<<grid, 256, 0, s>>>(n, b.gflag, b.gscan, b.sc, b.g_first);
 }
 
