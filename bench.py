@@ -445,6 +445,7 @@ def run_ours(args):
                            "of scalar and paired (f32x2) FMA chains "
                            "(MEASURED_PEAKS.json has no FP32 figure; its HBM copy peak is not the bound)",
             "algorithmic_flops_per_launch": alg_flops, "executed_flops_per_launch": exe_flops,
+            "executed_over_algorithmic": exe_flops / alg_flops,
             "reference_interactions_per_target": {"body_body": float(mean_pp),
                                                   "body_cell": float(mean_pc)},
             "executed_interactions_per_target": {"body_body": float(st[0]) / n,
