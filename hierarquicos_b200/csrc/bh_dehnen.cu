@@ -140,13 +140,18 @@ __global__ void roots_frontier_kernel(const SysScalars *__restrict__ ss, int nsy
 
 constexpr int kGenThreads = 256;            // threads of a block; one tile per block at a time
 constexpr int kGenItems = 4;                // consecutive input pairs per thread
+constexpr int kGenBlocksPerSm = 4;          // 64 registers a thread: 32 warps per SM hide the loads
 constexpr int kGenTile = kGenThreads * kGenItems;
 constexpr int kGenWarps = kGenThreads / kWarp;
+constexpr int kGenMutBits = 11;  // packed block scan: mutual count in the low bits
+constexpr int kGenMutMask = (1 << kGenMutBits) - 1;
+static_assert(kGenTile < (1 << kGenMutBits), "a tile's mutual pairs fit the low bits");
+static_assert((int64_t)kGenTile * 36 << kGenMutBits < (1ll << 31), "the packed count fits an int");
 // tile words of the chained scan: top 2 bits the state, low 62 bits the count
 constexpr uint64_t kGenAggregate = 1ull << 62;  // the tile's own count
 constexpr uint64_t kGenInclusive = 2ull << 62;  // sum of the counts of tiles 0..t
 constexpr uint64_t kGenValue = (1ull << 62) - 1;
-constexpr int64_t kGenSpins = 1 << 22;          // per word; about a second at most
+constexpr int64_t kGenSpins = 1 << 22;          // polls of one look-back; about a second at most
 
 __device__ __forceinline__ uint64_t gen_ld(const uint64_t *p) {
   uint64_t v;
@@ -181,33 +186,47 @@ __device__ __forceinline__ int gen_block_scan(int v, int *ws, int *total) {
   return before + x - v;
 }
 
-// Prefix of the counts of the tiles before tile t in one status list: publish
-// the tile's own count, then add up earlier tiles' words (an inclusive word
-// ends the walk).  Only tiles claimed earlier -- by blocks that are running
-// and publish before they wait -- are waited for, and every wait is bounded:
-// a wait that gives up raises kErrTimeout.
+// Prefix of the counts of the tiles before tile t in one status list, by one
+// whole warp: publish the tile's own count, then read the words of the 32
+// tiles before a window's end at once and add them up to the nearest
+// inclusive word (tile -1 counts as inclusive 0); a window with a word not yet
+// published is read again.  Only tiles claimed earlier -- by blocks that are
+// running and publish before they wait -- are waited for, and every wait is
+// bounded: a wait that gives up raises kErrTimeout.
 __device__ __forceinline__ int64_t gen_lookback(uint64_t *status, int t, int64_t count,
                                                 int *err) {
+  const int lane = threadIdx.x & (kWarp - 1);
   uint64_t *word = status + t;
   if (t == 0) {
-    gen_st(word, kGenInclusive | (uint64_t)count);
+    if (lane == 0) gen_st(word, kGenInclusive | (uint64_t)count);
     return 0;
   }
-  gen_st(word, kGenAggregate | (uint64_t)count);
+  if (lane == 0) gen_st(word, kGenAggregate | (uint64_t)count);
   int64_t excl = 0;
-  int j = t - 1;
+  int j = t - 1;  // the window is tiles j - 31 .. j, lane k reading tile j - k
   int64_t spins = 0;
-  while (j >= 0) {
-    const uint64_t w = gen_ld(status + j);
-    if ((w & ~kGenValue) == 0) {
-      if (++spins > kGenSpins) { atomicOr(err, kErrTimeout); break; }
+  for (;;) {
+    const int idx = j - lane;
+    const uint64_t w = idx >= 0 ? gen_ld(status + idx) : kGenInclusive;
+    const unsigned incl = __ballot_sync(0xffffffffu, (w & ~kGenValue) == kGenInclusive);
+    const unsigned unset = __ballot_sync(0xffffffffu, (w & ~kGenValue) == 0);
+    const int stop = incl ? __ffs(incl) - 1 : kWarp - 1;  // the last lane that counts
+    const unsigned counted = stop == kWarp - 1 ? 0xffffffffu : ((2u << stop) - 1u);
+    if (unset & counted) {
+      if (++spins > kGenSpins) {
+        if (lane == 0) atomicOr(err, kErrTimeout);
+        break;
+      }
       continue;
     }
-    excl += (int64_t)(w & kGenValue);
-    if ((w & ~kGenValue) == kGenInclusive) break;
-    --j;
+    int64_t v = lane <= stop ? (int64_t)(w & kGenValue) : 0;
+#pragma unroll
+    for (int o = kWarp / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    if (incl) break;
+    j -= kWarp;
   }
-  gen_st(word, kGenInclusive | (uint64_t)(excl + count));
+  if (lane == 0) gen_st(word, kGenInclusive | (uint64_t)(excl + count));
   return excl;
 }
 
@@ -269,7 +288,7 @@ __device__ __forceinline__ GenPair classify_pair(const Ent &e, int2 ab, double t
 // written by earlier generations.  The block of the last tile writes the two
 // new totals (the next generation's input count and the mutual count after
 // this generation).
-__global__ void __launch_bounds__(kGenThreads)
+__global__ void __launch_bounds__(kGenThreads, kGenBlocksPerSm)
 dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *__restrict__ nin,
                 int64_t cap_in, int2 *__restrict__ fout, unsigned long long *nout, int64_t cap_out,
                 int2 *__restrict__ mut, const unsigned long long *__restrict__ nmut_in,
@@ -307,17 +326,25 @@ dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *_
       n_out += g[q].kind == 1 ? g[q].k * (g[q].k + 1) / 2 : (g[q].kind == 3 ? g[q].k : 0);
       n_mut += g[q].kind == 2 ? 1 : 0;
     }
-    int tot_f, tot_m;
-    const int off_f = gen_block_scan(n_out, ws, &tot_f);
-    const int off_m = gen_block_scan(n_mut, ws, &tot_m);
-    if (threadIdx.x == 0) {
+    // one scan of both counts: a tile has at most kGenTile mutual pairs
+    // (< 2^kGenMutBits) and kGenTile * 36 new pairs, so the packed sum fits
+    int tot;
+    const int off = gen_block_scan((n_out << kGenMutBits) | n_mut, ws, &tot);
+    const int off_f = off >> kGenMutBits, off_m = off & kGenMutMask;
+    const int tot_f = tot >> kGenMutBits, tot_m = tot & kGenMutMask;
+    // the two chained scans, one warp each, at the same time
+    const int warp = threadIdx.x / kWarp;
+    if (warp == 0) {
       const int64_t ef = gen_lookback(status_f, t, tot_f, err);
+      if (threadIdx.x == 0) {
+        s_base[0] = ef;
+        if ((int64_t)t == ntiles - 1) *nout = (unsigned long long)(ef + tot_f);
+      }
+    } else if (warp == 1) {
       const int64_t em = gen_lookback(status_m, t, tot_m, err);
-      s_base[0] = ef;
-      s_base[1] = mut_base + em;
-      if ((int64_t)t == ntiles - 1) {
-        *nout = (unsigned long long)(ef + tot_f);
-        *nmut_out = (unsigned long long)(mut_base + em + tot_m);
+      if (threadIdx.x == kWarp) {
+        s_base[1] = mut_base + em;
+        if ((int64_t)t == ntiles - 1) *nmut_out = (unsigned long long)(mut_base + em + tot_m);
       }
     }
     __syncthreads();
@@ -358,15 +385,13 @@ dual_gen_kernel(Ent e, const int2 *__restrict__ fin, const unsigned long long *_
 // The mutual list is in a deterministic order, and the stable sort by target
 // keeps that order among a target's terms.
 __global__ void __launch_bounds__(256)
-expand_kernel(const int2 *__restrict__ mut, int64_t np, uint64_t *__restrict__ keys,
-              int32_t *__restrict__ vals, int32_t *cnt) {
+expand_kernel(const int2 *__restrict__ mut, int64_t np, uint2 *__restrict__ keys,
+              int2 *__restrict__ vals, int32_t *cnt) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t a = mut[i].x, b = mut[i].y;
-    keys[2 * (int64_t)i] = (uint64_t)(uint32_t)a;
-    vals[2 * (int64_t)i] = b;
-    keys[2 * (int64_t)i + 1] = (uint64_t)(uint32_t)b;
-    vals[2 * (int64_t)i + 1] = a;
+    keys[i] = make_uint2((uint32_t)a, (uint32_t)b);  // terms 2i (a <- b) and 2i + 1 (b <- a)
+    vals[i] = make_int2(b, a);
     atomicAdd(&cnt[a], 1);
     atomicAdd(&cnt[b], 1);
   }
@@ -677,22 +702,25 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
   if (grow(d.vals, d.vals_cap, 2 * (nh > 0 ? nh : 1)) != cudaSuccess) return 1;
   if (grow(d.hist, d.hist_cap, radix_hist_entries(nh > 0 ? nh : 1)) != cudaSuccess) return 1;
   cudaMemsetAsync(d.cnt, 0, (ne + 1) * sizeof(int32_t), s);
+  const int32_t *sources = d.vals;  // the terms' sources in target order
   if (np > 0) {
     const int g = grid_for(np, 256, 148 * 16);
-    expand_kernel<<<g, 256, 0, s>>>(d.mut, np, d.keys, d.vals, d.cnt);
+    expand_kernel<<<g, 256, 0, s>>>(d.mut, np, reinterpret_cast<uint2 *>(d.keys),
+                                    reinterpret_cast<int2 *>(d.vals), d.cnt);
     // stable by target: a target's terms keep the mutual list's order
-    radix_sort_pairs(d.keys, d.vals, d.keys + nh, d.vals + nh, nh, nullptr, bits_for64(ne), d.hist,
-                     &b.sc->err, s);
+    if (radix_sort_values32(d.keys, d.vals, d.keys + nh, d.vals + nh, nh, bits_for64(ne), d.hist,
+                            &b.sc->err, s) == 1)
+      sources = d.vals + nh;
   }
   exclusive_scan(d.cnt, d.beg, ne + 1, nullptr, nullptr, d.scan_tmp, &b.sc->err, s);
   const int egrid = grid_for(ne * kEvalLanes, 128, 148 * 32);
   const double G = p.G, eps2 = p.eps2;
   if (p.order >= 8)
-    eval_kernel<8><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
+    eval_kernel<8><<<egrid, 128, 0, s>>>(e, ne, d.beg, sources, G, eps2, d.F, d.H, d.T);
   else if (p.order >= 4)
-    eval_kernel<4><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
+    eval_kernel<4><<<egrid, 128, 0, s>>>(e, ne, d.beg, sources, G, eps2, d.F, d.H, d.T);
   else
-    eval_kernel<1><<<egrid, 128, 0, s>>>(e, ne, d.beg, d.vals, G, eps2, d.F, d.H, d.T);
+    eval_kernel<1><<<egrid, 128, 0, s>>>(e, ne, d.beg, sources, G, eps2, d.F, d.H, d.T);
   // downward pass and output: every body sums its ancestors' translated
   // expansions (cnt is free after the scan: it holds each body's parent node)
   int32_t *bp = d.cnt;

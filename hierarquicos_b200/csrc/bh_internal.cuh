@@ -149,6 +149,11 @@ inline int grid_for(int64_t n, int threads, int cap) {
 // kErrTimeout in *err (device).
 void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
                       const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s);
+// the same for 32-bit keys when only the values are wanted: the last pass
+// writes no keys and nothing is copied back; returns the buffer holding the
+// sorted values (0: v0, 1: v1)
+int radix_sort_values32(uint32_t *k0, int32_t *v0, uint32_t *k1, int32_t *v1, int64_t n, int bits,
+                        int32_t *hist, int *err, cudaStream_t s);
 // scratch of the scan, in int32 entries: a ticket and a 64-bit word per
 // 8192-value tile; scratch of the radix sort: digit counts of 8 passes x 256
 // digits, 8 tile counters, and a 64-bit word per (pass, 4096-key tile, digit)
@@ -198,7 +203,7 @@ struct DehnenBuffers {
   int2 *front = nullptr, *mut = nullptr;
   int64_t front_cap = 0, mut_cap = 0;
   int64_t want_front = 0, want_mut = 0;   // pairs per frontier buffer, mutual pairs
-  uint64_t *keys = nullptr;
+  uint32_t *keys = nullptr;               // one-sided terms: target (key), source (value)
   int32_t *vals = nullptr, *cnt = nullptr, *beg = nullptr, *hist = nullptr, *scan_tmp = nullptr;
   unsigned long long *counters = nullptr;
   int64_t keys_cap = 0, vals_cap = 0, cnt_cap = 0, beg_cap = 0, hist_cap = 0, scan_tmp_cap = 0,

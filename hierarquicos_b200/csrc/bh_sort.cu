@@ -72,8 +72,9 @@ __device__ int block_excl_scan(int v, int *ws, int *total) {
 
 // Digit histograms of all passes: ghist[p][d] = number of keys whose digit p
 // is d (warp-aggregated shared-memory counts, then one global add per bin).
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-digit_hist_kernel(const uint64_t *__restrict__ keys, int64_t n_max, const int32_t *n_dev,
+digit_hist_kernel(const K *__restrict__ keys, int64_t n_max, const int32_t *n_dev,
                   int passes, uint32_t *__restrict__ ghist) {
   __shared__ uint32_t h[kMaxPasses][kRadix];
   const int lane = threadIdx.x & (kWarp - 1);
@@ -85,7 +86,7 @@ digit_hist_kernel(const uint64_t *__restrict__ keys, int64_t n_max, const int32_
   for (int64_t base = (int64_t)blockIdx.x * kSortThreads; base < n; base += stride) {
     const int64_t idx = base + threadIdx.x;
     const bool valid = idx < n;
-    const uint64_t k = valid ? keys[idx] : 0ull;
+    const K k = valid ? keys[idx] : (K)0;
     for (int p = 0; p < passes; ++p) {
       const int d = valid ? (int)((k >> (8 * p)) & 0xff) : kRadix;
       const unsigned peers = __match_any_sync(0xffffffffu, d);
@@ -125,8 +126,9 @@ __device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+template <typename K>
 struct PassSmem {
-  uint64_t sk[kTile];
+  K sk[kTile];
   int32_t sv[kTile];
   int wh[kSortWarps][kRadix];
   int tile_start[kRadix];
@@ -135,13 +137,16 @@ struct PassSmem {
   int tile;
 };
 
+// kout may be null: the pass then writes only the values (a last pass whose
+// keys nobody reads).
+template <typename K>
 __global__ void __launch_bounds__(kSortThreads)
-onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vin,
-                uint64_t *__restrict__ kout, int32_t *__restrict__ vout, int64_t n_max,
+onesweep_kernel(const K *__restrict__ kin, const int32_t *__restrict__ vin,
+                K *__restrict__ kout, int32_t *__restrict__ vout, int64_t n_max,
                 const int32_t *n_dev, int shift, const uint32_t *__restrict__ gofs,
                 uint64_t *__restrict__ tiles, int32_t *__restrict__ tile_ctr, int *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  PassSmem &S = *reinterpret_cast<PassSmem *>(smem_raw);
+  PassSmem<K> &S = *reinterpret_cast<PassSmem<K> *>(smem_raw);
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   if (threadIdx.x == 0) S.tile = atomicAdd(tile_ctr, 1);
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
@@ -152,7 +157,7 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
   if (tile_base >= n) return;  // uniform across the block; later tiles return too
   const int tile_n = (int)bh_min64(kTile, n - tile_base);
 
-  uint64_t k[kItems];
+  K k[kItems];
   int32_t v[kItems];
   int dig[kItems], rank[kItems];
   const int wbase = warp * kWarp * kItems;
@@ -160,7 +165,7 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
   for (int i = 0; i < kItems; ++i) {
     int li = wbase + i * kWarp + lane;
     bool valid = li < tile_n;
-    k[i] = valid ? kin[tile_base + li] : 0ull;
+    k[i] = valid ? kin[tile_base + li] : (K)0;
     v[i] = valid ? vin[tile_base + li] : 0;
     dig[i] = valid ? (int)((k[i] >> shift) & 0xff) : kRadix;
   }
@@ -222,10 +227,10 @@ onesweep_kernel(const uint64_t *__restrict__ kin, const int32_t *__restrict__ vi
   }
   __syncthreads();
   for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
-    uint64_t key = S.sk[j];
-    int dd = (int)((key >> shift) & 0xff);
-    int64_t o = (int64_t)S.gbase[dd] + (j - S.tile_start[dd]);
-    kout[o] = key;
+    const K key = S.sk[j];
+    const int dd = (int)((key >> shift) & 0xff);
+    const int64_t o = (int64_t)S.gbase[dd] + (j - S.tile_start[dd]);
+    if (kout) kout[o] = key;
     vout[o] = S.sv[j];
   }
 }
@@ -332,7 +337,7 @@ regather_kernel(const uint64_t *__restrict__ k0, const int32_t *__restrict__ v0,
   }
 }
 
-bool g_sort_attr_set = false;
+bool g_sort_attr_set[2] = {false, false};
 
 }  // namespace
 
@@ -347,17 +352,21 @@ void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n
   scan_onepass_kernel<<<nb, kScanThreads, 0, s>>>(in, out, n, n_dev, tmp, total, total2, err);
 }
 
-void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
-                      const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s) {
-  if (!g_sort_attr_set) {
-    cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PassSmem));
-    g_sort_attr_set = true;
+// The passes of one sort; returns the buffer (0: k0/v0, 1: k1/v1) that holds
+// the result.  With keys_out false the last pass writes only the values.
+template <typename K>
+static int sort_passes(K *k0, int32_t *v0, K *k1, int32_t *v1, int64_t n, const int32_t *n_dev,
+                       int bits, int32_t *hist, int *err, bool keys_out, cudaStream_t s) {
+  bool &attr = g_sort_attr_set[sizeof(K) == 8 ? 1 : 0];
+  if (!attr) {
+    cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<K>));
+    attr = true;
   }
   const int64_t ntiles = (n + kTile - 1) / kTile;
   int passes = (bits + 7) / 8;
   if (passes < 1) passes = 1;
-  if (passes > kMaxPasses) passes = kMaxPasses;
+  if (passes > (int)sizeof(K)) passes = (int)sizeof(K);
   // scratch layout (int32 entries): digit counts [8][256], tile counters [8],
   // then the tile words (uint64) [passes][ntiles][256]
   uint32_t *ghist = reinterpret_cast<uint32_t *>(hist);
@@ -365,23 +374,34 @@ void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int6
   uint64_t *tiles = reinterpret_cast<uint64_t *>(hist + kMaxPasses * kRadix + kMaxPasses);
   const int64_t used = kMaxPasses * kRadix + kMaxPasses + 2 * (int64_t)passes * ntiles * kRadix;
   cudaMemsetAsync(hist, 0, used * sizeof(int32_t), s);
-  digit_hist_kernel<<<grid_for(n, kSortThreads, 148 * 8), kSortThreads, 0, s>>>(k0, n, n_dev,
-                                                                                passes, ghist);
+  digit_hist_kernel<K><<<grid_for(n, kSortThreads, 148 * 8), kSortThreads, 0, s>>>(k0, n, n_dev,
+                                                                                   passes, ghist);
   digit_scan_kernel<<<1, kSortThreads, 0, s>>>(ghist, passes);
-  uint64_t *ki = k0, *ko = k1;
+  K *ki = k0, *ko = k1;
   int32_t *vi = v0, *vo = v1;
   for (int p = 0; p < passes; ++p) {
-    onesweep_kernel<<<(unsigned)(ntiles > 0 ? ntiles : 1), kSortThreads, sizeof(PassSmem), s>>>(
-        ki, vi, ko, vo, n, n_dev, 8 * p, ghist + p * kRadix, tiles + (int64_t)p * ntiles * kRadix,
-        ctr + p, err);
-    uint64_t *tk = ki; ki = ko; ko = tk;
+    K *kw = (p == passes - 1 && !keys_out) ? nullptr : ko;
+    onesweep_kernel<K><<<(unsigned)(ntiles > 0 ? ntiles : 1), kSortThreads, sizeof(PassSmem<K>),
+                         s>>>(ki, vi, kw, vo, n, n_dev, 8 * p, ghist + p * kRadix,
+                              tiles + (int64_t)p * ntiles * kRadix, ctr + p, err);
+    K *tk = ki; ki = ko; ko = tk;
     int32_t *tv = vi; vi = vo; vo = tv;
   }
-  if (ki != k0) {
+  return ki == k0 ? 0 : 1;
+}
+
+void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int64_t n,
+                      const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s) {
+  if (sort_passes<uint64_t>(k0, v0, k1, v1, n, n_dev, bits, hist, err, true, s) == 1) {
     // odd number of passes: the result sits in the second buffer
-    cudaMemcpyAsync(k0, ki, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(v0, vi, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(k0, k1, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(v0, v1, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);
   }
+}
+
+int radix_sort_values32(uint32_t *k0, int32_t *v0, uint32_t *k1, int32_t *v1, int64_t n, int bits,
+                        int32_t *hist, int *err, cudaStream_t s) {
+  return sort_passes<uint32_t>(k0, v0, k1, v1, n, nullptr, bits, hist, err, false, s);
 }
 
 // The key sort orders all bodies of a batch by key; a stable sort by system
