@@ -16,8 +16,11 @@
 //    module holding it is loaded, until the process exits;
 //  * the first call on a device looks the array's device address up
 //    (cudaGetSymbolAddress, with that device current) and keeps it; later
-//    calls on that device reuse it.  Make that first call before any stream
-//    capture begins, so that the set-up does not happen inside one;
+//    calls on that device reuse it;
+//  * every call synchronises its stream (it reads the status back before
+//    returning), so it cannot be part of a stream capture: a call on a
+//    capturing stream is refused with BH_ERR_INVALID before anything is
+//    queued;
 //  * all calls on a device share the one array, which keeps the last call's
 //    contents; every call initialises what it reads.  Calls that overlap on
 //    the GPU (other streams, other host threads) race on that array: issue
@@ -156,6 +159,13 @@ extern "C" int bh_compute_forces_noalloc(const double *d_m, const double *d_x, c
     return bh_report_error(BH_ERR_INVALID,
                            "bh_compute_forces_noalloc: Dehnen's method sizes its pair lists at run "
                            "time and needs allocated work buffers; use a bh_system");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing((cudaStream_t)stream, &cap) != cudaSuccess)
+    return bh_report_error(BH_ERR_CUDA, "bh_compute_forces_noalloc: cudaStreamIsCapturing failed");
+  if (cap != cudaStreamCaptureStatusNone)
+    return bh_report_error(BH_ERR_INVALID,
+                           "bh_compute_forces_noalloc: the stream is being captured; the call "
+                           "synchronises its stream and cannot be captured");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return bh_report_error(BH_ERR_CUDA, "bh_compute_forces_noalloc: no current CUDA device");

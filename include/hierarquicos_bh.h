@@ -225,7 +225,9 @@ int bh_system_reference_targets(bh_system *sys, const bh_params *p, const int64_
  * comes from one fixed device array of about 7.9 MB inside the library, so n
  * is limited to BH_NOALLOC_MAX_N (larger n: BH_ERR_INVALID).  The first call on
  * a device looks that array up; all calls on a device share it, so calls that
- * overlap on the GPU race: run them one after another.  Synchronous. */
+ * overlap on the GPU race: run them one after another.  Synchronous: the call
+ * synchronises its stream, so it cannot be captured into a CUDA graph (a call
+ * on a capturing stream returns BH_ERR_INVALID and queues nothing). */
 #define BH_NOALLOC_MAX_N 8192
 int bh_compute_forces_noalloc(const double *d_m, const double *d_x, const double *d_y,
                               const double *d_z, int64_t n, const bh_params *p, double *d_out,

@@ -129,3 +129,32 @@ def test_noalloc_rejects_systems_above_its_limit():
                                        torch.cuda.current_stream().cuda_stream)
     assert rc == _lib.BH_ERR_INVALID
     assert str(_lib.BH_NOALLOC_MAX_N) in _lib.last_error()
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """The call synchronises its stream, so on a stream that is being captured
+    it returns BH_ERR_INVALID and queues nothing: the replayed graph holds only
+    the caller's own work."""
+    import torch
+
+    from hierarquicos_b200 import _lib
+
+    lib = _lib.lib()
+    n = 256
+    m, q = plummer(n, seed=24)
+    dm, dx, dy, dz = _device_arrays(m, q)
+    out = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    p = _lib.default_params()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        out.add_(1.0)
+        rc = lib.bh_compute_forces_noalloc(dm.data_ptr(), dx.data_ptr(), dy.data_ptr(),
+                                           dz.data_ptr(), n, C.byref(p), out.data_ptr(),
+                                           s.cuda_stream)
+    assert rc == _lib.BH_ERR_INVALID
+    assert "captur" in _lib.last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.all(out == 1.0)
