@@ -22,7 +22,10 @@ batching server against the plain single-system call:
     replay) with autotuned group/leaf parameters against a loop of plain
     calls;
   * dehnen -- Dehnen's dual-tree method (FP64) on the accuracy system, with its
-    error on the same targets.
+    error on the same targets;
+  * serving_sweep, parareal -- the serving config (Poisson arrivals, rate swept)
+    and the batched Parareal config, as ``--serving-sweep`` and ``--parareal``
+    print them on their own (single-GPU runs only).
 
 The RMS relative error is measured against the FP64 direct sum on 16,384
 seeded targets; served results are checked equal (bit for bit) to the plain
@@ -232,6 +235,61 @@ def dist_max(x, dev, world):
     return float(t.item())
 
 
+HOST_CPUS = None  # the process's CPUs before bind_to_gpu_node narrowed them
+
+
+def parse_cpulist(text):
+    """'0-3,8,10-11' -> {0, 1, 2, 3, 8, 10, 11}."""
+    cpus = set()
+    for part in text.strip().split(","):
+        if not part:
+            continue
+        lo, _, hi = part.partition("-")
+        cpus.update(range(int(lo), int(hi or lo) + 1))
+    return cpus
+
+
+def bind_to_gpu_node(torch, dev):
+    """Binds this process to the CPUs of the GPU's own NUMA node (the PCI
+    device's local_cpulist in sysfs), as a deployment pins a GPU's host
+    process: pinned host buffers allocated afterwards sit in that node's
+    memory, and host<->device copies do not cross the socket link (a copy from
+    the other socket's memory runs at a fraction of the bandwidth).  Returns
+    what was done, as a sentence for the bench line."""
+    global HOST_CPUS
+    try:
+        pr = torch.cuda.get_device_properties(dev)
+        addr = f"{pr.pci_domain_id:04x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        with open(f"/sys/bus/pci/devices/{addr}/local_cpulist") as fh:
+            local_cpus = parse_cpulist(fh.read())
+        current = os.sched_getaffinity(0)
+    except (OSError, AttributeError, ValueError, RuntimeError) as exc:
+        return f"unbound (GPU's node not known: {type(exc).__name__})"
+    mine = local_cpus & current
+    if not mine:
+        return "unbound (none of this process's CPUs is on the GPU's node)"
+    if mine == current:
+        return f"unbound: all {len(current)} CPUs of this process are on the GPU's node"
+    HOST_CPUS = current
+    os.sched_setaffinity(0, mine)
+    return (f"bound to the {len(mine)} CPUs of the GPU's node (sysfs local_cpulist); pinned "
+            f"buffers allocated afterwards")
+
+
+class all_host_cpus:
+    """Restores the process's full CPU set for the duration (child processes
+    started inside inherit it), then the narrowed one."""
+
+    def __enter__(self):
+        self.saved = os.sched_getaffinity(0)
+        if HOST_CPUS:
+            os.sched_setaffinity(0, HOST_CPUS)
+        return self
+
+    def __exit__(self, *a):
+        os.sched_setaffinity(0, self.saved)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -244,6 +302,7 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    bound_cpus = bind_to_gpu_node(torch, local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     dev = torch.device("cuda", local)
@@ -454,9 +513,10 @@ def run_ours(args):
             "fp32_paired_fma_tflops": peak[2] / 1e3, "fp64_peak_tflops": peak[1] / 1e3}
 
         # ---- end to end from pinned host buffers ----
-        hm = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        hx, hy, hz = (torch.empty_like(hm) for _ in range(3))
+        # each array pinned on its own (empty_like would not keep pin_memory)
+        hm, hx, hy, hz = (torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(4))
         hout = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
+        assert all(h.is_pinned() for h in (hm, hx, hy, hz, hout))
         for h, d in zip((hm, hx, hy, hz), systems[0]):
             h.copy_(d.cpu())
         L = _lib.lib()
@@ -518,9 +578,12 @@ def run_ours(args):
                        "ms_per_step": served_e2e_ms, "h2d_bytes_per_step": 4 * 8 * n,
                        "d2h_bytes_per_step": 3 * 8 * n,
                        "api": "serving.Server with host requests (pinned in, results copied out)",
+                       "host_cpus": bound_cpus,
                        "p50_ms": hmet["p50_ms"], "p99_ms": hmet["p99_ms"],
                        "equal_to_plain_bitwise": same_host,
                        "plain": {"value": world * n / (plain_e2e_ms * 1e-3), "ms_per_step": plain_e2e_ms,
+                                 "ms_min": min(te), "ms_median": statistics.median(te),
+                                 "ms_max": max(te),
                                  "api": "bh_compute_forces_ex (pinned host arrays)"},
                        "plain_pageable": {"value": world * n / (pageable_ms * 1e-3),
                                           "ms_per_step": pageable_ms,
@@ -533,6 +596,14 @@ def run_ours(args):
 
         if rank == 0 and world == 1:
             line["cpu_baseline"] = cpu_baseline(n, args.order)
+            # the serving and Parareal configs, each recorded beside the
+            # headline; a failure there is reported, not fatal to the line
+            for key, fn in (("serving_sweep", lambda: serving_sweep(args, local)),
+                            ("parareal", lambda: parareal_summary(args))):
+                try:
+                    line[key] = fn()
+                except Exception as exc:  # noqa: BLE001
+                    line[key] = {"error": f"{type(exc).__name__}: {exc}"[:500]}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -709,11 +780,12 @@ def cpu_baseline_runs(n, order, runs, warmup, seed=1000):
     summary with the per-run times."""
     from oracle.cpu_baseline import child_env, usable_cores
 
-    cores = usable_cores()
-    r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n), "--runs",
-                        str(runs), "--warmup", str(warmup), "--order", str(order), "--seed",
-                        str(seed), "--theta", str(THETA), "--eps", str(EPS)],
-                       env=child_env(cores), cwd=ROOT, capture_output=True, text=True)
+    with all_host_cpus():  # the CPU arm gets every core of the host
+        cores = usable_cores()
+        r = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", "--n", str(n), "--runs",
+                            str(runs), "--warmup", str(warmup), "--order", str(order), "--seed",
+                            str(seed), "--theta", str(THETA), "--eps", str(EPS)],
+                           env=child_env(cores), cwd=ROOT, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"CPU baseline failed ({r.returncode}): {r.stderr[-2000:]}")
     for line in r.stdout.splitlines()[::-1]:
@@ -798,13 +870,20 @@ def run_serving_sweep(args):
     forces/s over the run."""
     import torch
 
-    from hierarquicos_b200 import _lib, serving
-    from hierarquicos_b200.initial_values import generate_initial_values_device
-
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if int(os.environ.get("RANK", "0")) != 0:
         return
     torch.cuda.set_device(local)
+    print(json.dumps(serving_sweep(args, local)), flush=True)
+
+
+def serving_sweep(args, local):
+    """The serving config's line (see run_serving_sweep) as a dict."""
+    import torch
+
+    from hierarquicos_b200 import _lib, serving
+    from hierarquicos_b200.initial_values import generate_initial_values_device
+
     p = _lib.default_params(theta=THETA, eps=EPS, order=args.order, mac=args.mac)
     if args.pipeline is not None:
         p.pipeline = args.pipeline
@@ -857,7 +936,7 @@ def run_serving_sweep(args):
                       "wall_s": met["wall_s"], "requests": met["requests"],
                       "by_kind": met["by_kind"], "paused_ticks": met["paused_ticks"]})
     sizes = [int(sp[0].numel()) for sp in specs]
-    print(json.dumps({
+    return {
         "metric": "serving: Poisson arrivals, rate swept (p50/p99 latency ms, forces/s)",
         "config": {"workload": "force and leapfrog requests (1-100 steps, dt 1e-3), N log-uniform "
                                "in [1024, 2^21], Plummer / Hernquist / uniform sphere, device "
@@ -870,7 +949,7 @@ def run_serving_sweep(args):
                      "p50_ms": cap["p50_ms"], "p99_ms": cap["p99_ms"], "by_kind": cap["by_kind"]},
         "scheduling": "force requests admitted before integrations; a tick holding force "
                       "requests takes integrations up to 2^22 bodies (at most 8 ticks out in a row)",
-        "rates": rates}), flush=True)
+        "rates": rates}
 
 
 def run_parareal(args):
@@ -888,12 +967,19 @@ def run_parareal(args):
     distance of the Parareal end state from it."""
     import torch
 
-    from hierarquicos_b200 import parareal as pr
-    from hierarquicos_b200.initial_values import generate_initial_values
-
     if int(os.environ.get("RANK", "0")) != 0:
         return
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    print(json.dumps(parareal_summary(args)), flush=True)
+
+
+def parareal_summary(args):
+    """The batched Parareal config's line (see run_parareal) as a dict."""
+    import torch
+
+    from hierarquicos_b200 import parareal as pr
+    from hierarquicos_b200.initial_values import generate_initial_values
+
     n, W, tf, G, eps = args.parareal_bodies, 64, 1.0, 1.0, 0.01
     m, q, p = generate_initial_values(n, -1.0, -1.0, True, False, "plummer", (1.0, 1.0), seed=4,
                                       velocities=True)
@@ -929,7 +1015,7 @@ def run_parareal(args):
                      "speedup_to_convergence": (seq_s / res.seconds) if res.converged else None,
                      "time_to_1e-12_s": time_to(1e-12), "time_to_1e-20_s": time_to(1e-20),
                      "end_state_vs_sequential_fine": float(np.sqrt(np.sum(d * d))) / (6 * n)})
-    print(json.dumps({
+    return {
         "metric": "batched Parareal: error per iteration (reference norm), s per iteration, "
                   "speed-up over the sequential fine run",
         "config": {"workload": f"plummer N={n} b=1 equal masses seeded, velocity Verlet, {W} slices "
@@ -937,7 +1023,7 @@ def run_parareal(args):
                                "2 steps per slice (dt 1/128)",
                    "fine": "velocity Verlet, quadrupole theta 0.3, 16 steps per slice (dt 1/1024)",
                    "eps": eps, "G": G, "tolerance": 1e-20, "max_iterations": args.parareal_iters},
-        "runs": runs}), flush=True)
+        "runs": runs}
 
 
 def main():

@@ -51,6 +51,8 @@ struct bh_system {
   // first use
   cudaStream_t copy_st[3] = {nullptr, nullptr, nullptr};
   cudaEvent_t copy_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // pageable host arrays: staged by host threads through pinned slots
+  bh::HostCopy *hcopy = nullptr;
 };
 
 namespace {
@@ -464,7 +466,15 @@ int default_system(bh_system **out) {
   return BH_OK;
 }
 
-// copies host arrays into the default system's staging buffers
+int ensure_hostcopy(bh_system *s) {
+  if (!s->hcopy) s->hcopy = bh::hostcopy_create(s->device);
+  if (!s->hcopy) return set_err(BH_ERR_CUDA, "host staging: %s", cudaGetErrorString(cudaGetLastError()));
+  return BH_OK;
+}
+
+// copies host arrays into the default system's staging buffers: pinned
+// arrays straight from the caller's memory, pageable ones through the host
+// staging threads
 int stage_inputs(bh_system *s, const double *m, const double *x, const double *y,
                  const double *z, int64_t n, cudaStream_t st) {
   const int64_t off[2] = {0, n};
@@ -473,6 +483,21 @@ int stage_inputs(bh_system *s, const double *m, const double *x, const double *y
   rc = ensure_host_staging(s, n);
   if (rc) return rc;
   Buffers &b = s->b;
+  const double *in[4] = {m, x, y, z};
+  bool pinned = true;
+  for (const double *a : in) {
+    const bh::HostKind k = bh::host_kind(a);
+    if (k == bh::HostKind::kDevice)
+      return set_err(BH_ERR_INVALID, "a device pointer was passed where host arrays are expected");
+    pinned = pinned && k == bh::HostKind::kPinned;
+  }
+  if (!pinned) {
+    rc = ensure_hostcopy(s);
+    if (rc) return rc;
+    double *dst[4] = {b.hm, b.hx, b.hy, b.hz};
+    BH_CUDA(bh::hostcopy_upload(s->hcopy, in, dst, 4, n, st));
+    return BH_OK;
+  }
   if (!s->copy_ev[0]) {
     for (int k = 0; k < 3; ++k)
       BH_CUDA(cudaStreamCreateWithFlags(&s->copy_st[k], cudaStreamNonBlocking));
@@ -574,6 +599,7 @@ int bh_system_destroy(bh_system *s) {
     if (s->copy_st[k]) cudaStreamDestroy(s->copy_st[k]);
   for (int k = 0; k < 4; ++k)
     if (s->copy_ev[k]) cudaEventDestroy(s->copy_ev[k]);
+  bh::hostcopy_destroy(s->hcopy);
   delete s;
   return BH_OK;
 }
@@ -835,6 +861,9 @@ int bh_compute_forces_ex(const double *m, const double *x, const double *y, cons
   rc = default_system(&s);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  const bh::HostKind ok = bh::host_kind(out);
+  if (ok == bh::HostKind::kDevice)
+    return set_err(BH_ERR_INVALID, "a device pointer was passed as the host result array");
   rc = stage_inputs(s, m, x, y, z, n, st);
   if (rc) return rc;
   Buffers &b = s->b;
@@ -842,6 +871,16 @@ int bh_compute_forces_ex(const double *m, const double *x, const double *y, cons
   if (rc) return rc;
   rc = bh_system_walk(s, p, b.hout, stream);
   if (rc) return rc;
+  if (ok != bh::HostKind::kPinned) {
+    // pageable result: the status first (it may redo the walk), then the
+    // staged copy, which returns when the caller's array is written
+    rc = finish(s, st);
+    if (rc) return rc;
+    rc = ensure_hostcopy(s);
+    if (rc) return rc;
+    BH_CUDA(bh::hostcopy_download(s->hcopy, out, b.hout, 3 * n, st));
+    return BH_OK;
+  }
   // the result's copy goes on the stream before the status is read, so it
   // follows the walk without a host round trip; if the status check redoes
   // the walk (strict-key rebuild, larger stack) the copy is made again
@@ -879,11 +918,20 @@ int bh_compute_forces_direct(const double *m, const double *x, const double *y,
   int rc = default_system(&s);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  const bh::HostKind ok = bh::host_kind(out);
+  if (ok == bh::HostKind::kDevice)
+    return set_err(BH_ERR_INVALID, "a device pointer was passed as the host result array");
   rc = stage_inputs(s, m, x, y, z, n, st);
   if (rc) return rc;
   Buffers &b = s->b;
   bh::launch_direct(b.hm, b.hx, b.hy, b.hz, n, nullptr, 0, G, eps * eps, out_kind, b.hout, st);
   BH_CUDA(cudaGetLastError());
+  if (ok != bh::HostKind::kPinned) {
+    rc = ensure_hostcopy(s);
+    if (rc) return rc;
+    BH_CUDA(bh::hostcopy_download(s->hcopy, out, b.hout, 3 * n, st));
+    return BH_OK;
+  }
   BH_CUDA(cudaMemcpyAsync(out, b.hout, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
   BH_CUDA(cudaStreamSynchronize(st));
   return BH_OK;

@@ -143,6 +143,22 @@ inline int grid_for(int64_t n, int threads, int cap) {
   return (int)g;
 }
 
+// Host-array transfers through a pool of host threads and pinned slots
+// (bh_hostcopy.cu): pageable arrays are staged chunk by chunk while the copy
+// engines move the neighbouring chunks.
+enum class HostKind { kPageable, kPinned, kDevice };
+HostKind host_kind(const void *p);
+struct HostCopy;
+HostCopy *hostcopy_create(int device);  // nullptr when a CUDA call failed
+void hostcopy_destroy(HostCopy *h);
+// count host arrays of n doubles into device arrays; st waits for them
+cudaError_t hostcopy_upload(HostCopy *h, const double *const *src, double *const *dst, int count,
+                            int64_t n, cudaStream_t st);
+// n doubles of device memory into a host array after the work queued on st;
+// returns when the host array is written
+cudaError_t hostcopy_download(HostCopy *h, double *dst, const double *src, int64_t n,
+                              cudaStream_t st);
+
 // stable LSD radix sort of (key, value) pairs over bits [0, bits); the
 // result ends in (k0, v0).  n_dev, when given, holds the element count on the
 // device (n is then an upper bound).  A look-back wait that gives up sets

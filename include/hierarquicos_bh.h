@@ -85,7 +85,11 @@ int bh_last_error(char *buf, int len);
 /* Drop-in for api_mod.compute_forces (fortran/api3d.f90:20-41; REAL(16) twin
  * parareal/api3d.f90:20-44): host arrays in, forces (N,3) out, every call a
  * fresh tree.  order: 1 monopole, 4 quadrupole (the f2py quad=.TRUE.), 8
- * octupole.  out_kind 0 forces, 1 accelerations. */
+ * octupole.  out_kind 0 forces, 1 accelerations.  Host arrays may be pinned
+ * (copied straight by the copy engines, overlapped on several streams) or
+ * ordinary pageable memory (staged through pinned chunks by a pool of host
+ * threads while the copy engines move the neighbouring chunks); a device
+ * pointer is refused (BH_ERR_INVALID).  Returns when out is written. */
 int bh_compute_forces(const double *m, const double *x, const double *y, const double *z,
                       int64_t n, double theta, double G, double eps, int order, int out_kind,
                       double *out, void *stream);

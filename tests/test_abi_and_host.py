@@ -113,3 +113,34 @@ def test_error_stats():
     f = fd * (1 + 1e-3)
     s = error_stats(f, fd)
     assert abs(s["rms_rel"] - 1e-3) < 1e-9 and abs(s["max_rel"] - 1e-3) < 1e-9
+
+
+def test_bench_cpu_binding_helpers():
+    """The bench's NUMA binding: sysfs cpulist parsing, no change without a
+    GPU, and the full CPU set restored around the CPU arm's child process."""
+    import os
+    import sys
+
+    import torch
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+
+    assert bench.parse_cpulist("0-3,8,10-11\n") == {0, 1, 2, 3, 8, 10, 11}
+    assert bench.parse_cpulist("5") == {5}
+    before = os.sched_getaffinity(0)
+    if not torch.cuda.is_available():
+        assert bench.bind_to_gpu_node(torch, 0).startswith("unbound")
+        assert os.sched_getaffinity(0) == before
+    saved = bench.HOST_CPUS
+    try:
+        one = {min(before)}
+        bench.HOST_CPUS = before
+        os.sched_setaffinity(0, one)
+        with bench.all_host_cpus():
+            assert os.sched_getaffinity(0) == before
+        assert os.sched_getaffinity(0) == one
+    finally:
+        bench.HOST_CPUS = saved
+        os.sched_setaffinity(0, before)
