@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 import torch
 
-from ._lib import BHParams, check, default_params, lib
+from ._lib import BH_ERR_NOT_BUILT, BHError, BHParams, check, default_params, lib
 from .system import BHSystem, _dptr, _stream, offsets_of
 
 
@@ -80,19 +80,56 @@ def _rows(a, dev) -> torch.Tensor:
 
 class ForceField:
     """Forces of a batch: Barnes-Hut (``kind='bh'``) or FP64 direct sum
-    (``kind='direct'``), written in the walk's per-system block layout."""
+    (``kind='direct'``), written in the walk's per-system block layout.
 
-    def __init__(self, kind: str = "bh", params: BHParams | None = None, device=None, **kw):
+    With ``graph=True`` a Barnes-Hut field records its build + walk into a CUDA
+    graph after the first evaluation of a state and replays it while it is
+    called with the same state tensors, layout and output (an integrator
+    stepping one state): one launch instead of one per kernel, for the small
+    systems whose evaluation is launch-bound.  Every replay is followed by the
+    same status check (strict keys, stack growth) as a plain call, and gives
+    the same bits.  The graph writes into a buffer of the field's own, which
+    is copied into the caller's output."""
+
+    def __init__(self, kind: str = "bh", params: BHParams | None = None, device=None,
+                 graph: bool = False, **kw):
         if kind not in ("bh", "direct"):
             raise ValueError("kind must be 'bh' or 'direct'")
         self.kind = kind
         self.params = params if params is not None else default_params(**kw)
         self.sys = BHSystem(as_device(device).index) if kind == "bh" else None
+        self.graph = graph and kind == "bh"
+        self._graph_key = None
+        self._graph_out = None
 
     def __call__(self, st: BatchState, out: torch.Tensor) -> torch.Tensor:
         x, y, z = st.q[0], st.q[1], st.q[2]
         if self.kind == "bh":
-            return self.sys.forces_batch(st.m, x, y, z, st.offsets, self.params, out=out)
+            if not self.graph:
+                return self.sys.forces_batch(st.m, x, y, z, st.offsets, self.params, out=out)
+            # the graph writes into the field's own buffer (callers often hand
+            # a fresh output per call), copied out afterwards
+            key = (st.m.data_ptr(), x.data_ptr(), y.data_ptr(), z.data_ptr(), st.n,
+                   st.offsets.tobytes())
+            if key == self._graph_key:
+                try:
+                    self.sys.replay()
+                except BHError as e:
+                    # a workspace that grew since (stack, layout) dropped the
+                    # graph: evaluate normally and record it again
+                    if e.code != BH_ERR_NOT_BUILT:
+                        raise
+                else:
+                    self.sys.sync()
+                    out.copy_(self._graph_out)
+                    return out
+            if self._graph_out is None or self._graph_out.numel() != 3 * st.n:
+                self._graph_out = torch.empty(3 * st.n, dtype=torch.float64, device=out.device)
+            self.sys.forces_batch(st.m, x, y, z, st.offsets, self.params, out=self._graph_out)
+            self.sys.capture(self.params, self._graph_out)  # the next call replays it
+            self._graph_key = key
+            out.copy_(self._graph_out)
+            return out
         p = self.params
         for s in range(st.nsys):
             a, b = int(st.offsets[s]), int(st.offsets[s + 1])

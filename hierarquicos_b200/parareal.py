@@ -48,10 +48,10 @@ class Propagator:
     order: int = 4
     precision: int = 0
 
-    def field(self, G: float, eps: float, device=None) -> ForceField:
+    def field(self, G: float, eps: float, device=None, graph: bool = False) -> ForceField:
         p = default_params(theta=self.theta, G=G, eps=eps, order=self.order,
                            precision=self.precision)
-        return ForceField(self.kind, p, device)
+        return ForceField(self.kind, p, device, graph=graph)
 
     def run(self, st: BatchState, field: ForceField, window: float) -> None:
         dt = window / self.steps
@@ -137,7 +137,9 @@ def integrate_parareal(m, q0, p0, tf: float, num_windows: int, n_itermax: int, t
     n = m.size
     W = num_windows
     window = tf / W
-    cfield = coarse.field(G, eps, dev)
+    # the coarse propagator steps one scratch state window after window:
+    # its evaluations replay one recorded graph
+    cfield = coarse.field(G, eps, dev, graph=True)
     ffield = fine.field(G, eps, dev)
 
     # U[k]: all windows' starting states, one batch of W systems
@@ -240,7 +242,7 @@ def sequential_fine(m, q0, p0, tf: float, num_windows: int, fine: Propagator, G:
     dev = as_device(device)
     m = np.ascontiguousarray(m, np.float64)
     st = BatchState.single(m, np.asarray(q0, np.float64).T, np.asarray(p0, np.float64).T, dev)
-    field = fine.field(G, eps, dev)
+    field = fine.field(G, eps, dev, graph=True)  # one state stepped throughout: replayed
     qs, ps = [st.q.T.cpu().numpy()], [st.p.T.cpu().numpy()]
     for _ in range(num_windows - 1):
         fine.run(st, field, tf / num_windows)

@@ -132,6 +132,38 @@ def test_batch_integration_equals_single(ig):
         assert np.array_equal(pb, one.p.T.cpu().numpy())
 
 
+def test_graph_replayed_field_follows_the_plain_trajectory(ig):
+    """A field that replays its recorded build + walk gives the plain field's
+    trajectory bit for bit: velocity Verlet on a batch, and symplectic Euler on
+    one scratch state refilled between windows (the Parareal coarse sweep)."""
+    parts = [plummer_state(n, seed=40 + n) for n in (3000, 1200)]
+    off = ig.offsets_of([len(a[0]) for a in parts])
+    args = (np.concatenate([a[0] for a in parts]), np.concatenate([a[1] for a in parts]).T,
+            np.concatenate([a[2] for a in parts]).T, off)
+    runs = []
+    for graph in (False, True):
+        st = ig.BatchState(*args)
+        field = ig.ForceField("bh", theta=0.6, eps=0.01, order=4, graph=graph)
+        ig.verlet(st, field, 6, 1e-3)
+        runs.append((st.q.cpu().numpy(), st.p.cpu().numpy()))
+    assert np.array_equal(runs[0][0], runs[1][0]) and np.array_equal(runs[0][1], runs[1][1])
+
+    m, q, p = plummer_state(2500, seed=47)
+    ends = []
+    for graph in (False, True):
+        one = ig.BatchState.single(m, q.T, p.T)
+        field = ig.ForceField("bh", theta=0.8, eps=0.01, order=1, graph=graph)
+        seen = []
+        for w in range(3):
+            if w:  # the next window starts from a perturbed copy, in the same tensors
+                one.q.copy_(one.q * (1.0 + 1e-3 * w))
+            ig.symplectic_euler(one, field, 2, 1e-2)
+            seen.append((one.q.cpu().numpy(), one.p.cpu().numpy()))
+        ends.append(seen)
+    for (qa, pa), (qb, pb) in zip(*ends):
+        assert np.array_equal(qa, qb) and np.array_equal(pa, pb)
+
+
 def test_parareal_matches_oracle_direct(ig, oracle_mod):
     """The reference's Parareal with direct-force propagators, device against
     the CPU restatement: same iterates (to FP64 rounding of the force sums)
