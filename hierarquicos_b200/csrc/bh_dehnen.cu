@@ -33,6 +33,8 @@
 //       hess   += M_s D2,  third += M_s D3           (r^2 = R^2 + eps^2)
 //       field  += (octupole) 0.5 (3 G r^-5 c - 15 G r^-7 C:RR) / M_t,
 //                 C_jkl = M_s O_t,jkl - M_t O_s,jkl, c_j = C_jkk
+//                 (summed over the target's terms, then halved and divided
+//                 by M_t once)
 //     which is the reference's update of both nodes written once per side.
 //     Terms between coincident points without softening (r = 0) are skipped.
 //  4. Downward pass (dehnen_forces :1560-1673): child field += parent field +
@@ -55,6 +57,7 @@ struct Ent {
   const double4 *com;
   const double4 *spos;
   const double *quad;
+  const double *squad;  // quad / mass per node (order >= 4)
   const double *oct;
   const double *rmax;
   int64_t n;  // bodies: entity n + p is body p
@@ -126,6 +129,19 @@ rmax_fused_kernel(const Scalars *__restrict__ scr, Ent e, const int32_t *__restr
       __threadfence();
       j = p;
     }
+  }
+}
+
+// Every node's quadrupole divided by its mass, once, for the terms that use
+// it as a source (the same correctly rounded quotients the terms would form).
+__global__ void __launch_bounds__(256)
+spec_quad_kernel(const Scalars *__restrict__ scr, const double4 *__restrict__ com,
+                 const double *__restrict__ quad, double *__restrict__ squad) {
+  const int M = scr->n_compact;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
+    const double m = com[j].w;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) squad[6 * (int64_t)j + q] = m != 0.0 ? quad[6 * (int64_t)j + q] / m : 0.0;
   }
 }
 
@@ -397,17 +413,19 @@ expand_kernel(const int2 *__restrict__ mut, int64_t np, uint2 *__restrict__ keys
   }
 }
 
-// One one-sided term (t <- s) added to f (3), h (6), tt (10).
+// One one-sided term (t <- s; cs the source's centre of mass and mass) added
+// to f (3), h (6), tt (10); the octupole torque term (order 8) goes to tq (3)
+// without its 0.5 / M_t factor, which the caller applies once to the
+// target's sum.
 template <int ORDER>
 __device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 &ct, bool tnode,
                                          int64_t s, double G, double eps2, double *f, double *h,
-                                         double *tt) {
-  const double4 cs = ent_com(e, s);
+                                         double *tt, double *tq, const double4 cs) {
   const double Ms = cs.w, Mt = ct.w;
   const double dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
   const double r2 = dx * dx + dy * dy + dz * dz + eps2;
   if (r2 == 0.0) return;
-  const double rinv = 1.0 / sqrt(r2);
+  const double rinv = rsqrt(r2);
   const double rinv2 = rinv * rinv;
   const double rinv3 = rinv * rinv2;
   const double D1x = -G * dx * rinv3, D1y = -G * dy * rinv3, D1z = -G * dz * rinv3;
@@ -434,10 +452,9 @@ __device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 
   D3[8] = G * (-15.0 * dy * dz * dz * rinv7 + 3.0 * dy * rinv5);
   D3[9] = G * (-15.0 * dz * dz * dz * rinv7 + 9.0 * dz * rinv5);
   double cq[3] = {0.0, 0.0, 0.0};
-  if (s < e.n) {  // a node's specific quadrupole; a body has none
-    const double *q = e.quad + 6 * s;
-    const double Q0 = q[0] / Ms, Q1 = q[1] / Ms, Q2 = q[2] / Ms, Q3 = q[3] / Ms, Q4 = q[4] / Ms,
-                 Q5 = q[5] / Ms;
+  if (s < e.n) {  // a node's specific quadrupole (divided once per node); a body has none
+    const double *q = e.squad + 6 * s;
+    const double Q0 = q[0], Q1 = q[1], Q2 = q[2], Q3 = q[3], Q4 = q[4], Q5 = q[5];
     cq[0] = Q0 * D3[0] + 2.0 * Q3 * D3[1] + 2.0 * Q4 * D3[2] + Q1 * D3[3] + 2.0 * Q5 * D3[4] +
             Q2 * D3[5];
     cq[1] = Q0 * D3[1] + 2.0 * Q3 * D3[3] + 2.0 * Q4 * D3[4] + Q1 * D3[6] + 2.0 * Q5 * D3[7] +
@@ -469,9 +486,9 @@ __device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 
     const double crz = C[6] * dx * dx + C[7] * dy * dy + C[8] * dz * dz +
                        2.0 * (C[9] * dx * dy + C[2] * dx * dz + C[5] * dy * dz);
     const double a3 = 3.0 * G * rinv5, a15 = 15.0 * G * rinv7;
-    f[0] = f[0] + 0.5 * (a3 * cx - a15 * crx) / Mt;
-    f[1] = f[1] + 0.5 * (a3 * cy - a15 * cry) / Mt;
-    f[2] = f[2] + 0.5 * (a3 * cz - a15 * crz) / Mt;
+    tq[0] = tq[0] + (a3 * cx - a15 * crx);
+    tq[1] = tq[1] + (a3 * cy - a15 * cry);
+    tq[2] = tq[2] + (a3 * cz - a15 * crz);
   }
 }
 
@@ -489,7 +506,7 @@ __global__ void __launch_bounds__(128)
 eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const int32_t *__restrict__ src,
             double G, double eps2, double *__restrict__ F, double *__restrict__ H,
             double *__restrict__ T) {
-  constexpr int NV = ORDER >= 4 ? 19 : 3;
+  constexpr int NV = ORDER >= 8 ? 22 : (ORDER >= 4 ? 19 : 3);  // f, h, tt[, torque]
   constexpr int kPerWarp = kWarp / kEvalLanes;
   const int lane = threadIdx.x & (kWarp - 1);
   const int sub = lane / kEvalLanes, sl = lane % kEvalLanes;
@@ -497,16 +514,33 @@ eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const int32_t *_
   const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) / kWarp;
   for (int64_t t0 = warp_id * kPerWarp; t0 < ne; t0 += wstride * kPerWarp) {
     const int64_t t = t0 + sub;
-    double v[19];
+    double v[22];
 #pragma unroll
-    for (int q = 0; q < 19; ++q) v[q] = 0.0;
+    for (int q = 0; q < 22; ++q) v[q] = 0.0;
     if (t < ne) {
       const int kb = beg[t], ke = beg[t + 1];
       if (kb < ke) {
         const double4 ct = ent_com(e, t);
         const bool tnode = t < e.n;
-        for (int k = kb + sl; k < ke; k += kEvalLanes)
-          add_term<ORDER>(e, t, ct, tnode, (int64_t)src[k], G, eps2, v, v + 3, v + 9);
+        if (ORDER < 8) {
+          // the next term's source and centre of mass load while this one
+          // is computed (the octupole term needs those registers itself)
+          int k = kb + sl;
+          int64_t sn = k < ke ? (int64_t)src[k] : 0;
+          double4 cn = k < ke ? ent_com(e, sn) : make_double4(0.0, 0.0, 0.0, 0.0);
+          while (k < ke) {
+            const int64_t sc = sn;
+            const double4 cc = cn;
+            k += kEvalLanes;
+            if (k < ke) { sn = (int64_t)src[k]; cn = ent_com(e, sn); }
+            add_term<ORDER>(e, t, ct, tnode, sc, G, eps2, v, v + 3, v + 9, v + 19, cc);
+          }
+        } else {
+          for (int k = kb + sl; k < ke; k += kEvalLanes) {
+            const int64_t sc = (int64_t)src[k];
+            add_term<ORDER>(e, t, ct, tnode, sc, G, eps2, v, v + 3, v + 9, v + 19, ent_com(e, sc));
+          }
+        }
       }
     }
     // every lane of the warp takes part (lanes past ne hold zeros)
@@ -516,6 +550,11 @@ eval_kernel(Ent e, int64_t ne, const int32_t *__restrict__ beg, const int32_t *_
       for (int o = kEvalLanes / 2; o > 0; o >>= 1) v[q] = v[q] + __shfl_xor_sync(0xffffffffu, v[q], o);
     }
     if (sl == 0 && t < ne) {
+      if (ORDER >= 8 && (v[19] != 0.0 || v[20] != 0.0 || v[21] != 0.0)) {
+        const double Mt = ent_com(e, t).w;  // > 0: terms with a massless member are dropped
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = v[q] + 0.5 * v[19 + q] / Mt;
+      }
 #pragma unroll
       for (int q = 0; q < 3; ++q) F[3 * t + q] = v[q];
       if (ORDER >= 4) {
@@ -627,8 +666,8 @@ int bits_for64(int64_t v) {
 }  // namespace
 
 void free_dehnen(DehnenBuffers &d) {
-  void *ptrs[] = {d.rmax, d.F, d.H, d.T, d.front, d.mut, d.keys, d.vals, d.cnt, d.beg, d.hist,
-                  d.scan_tmp, d.counters, d.gen_status, d.gen_tiles};
+  void *ptrs[] = {d.rmax, d.F, d.H, d.T, d.squad, d.front, d.mut, d.keys, d.vals, d.cnt, d.beg,
+                  d.hist, d.scan_tmp, d.counters, d.gen_status, d.gen_tiles};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   d = DehnenBuffers();
@@ -641,6 +680,7 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
   if (grow(d.F, d.F_cap, 3 * ne) != cudaSuccess) return 1;
   if (p.order >= 4 && grow(d.H, d.H_cap, 6 * ne) != cudaSuccess) return 1;
   if (p.order >= 4 && grow(d.T, d.T_cap, 10 * ne) != cudaSuccess) return 1;
+  if (p.order >= 4 && grow(d.squad, d.squad_cap, 6 * n) != cudaSuccess) return 1;
   if (grow(d.cnt, d.cnt_cap, ne + 1) != cudaSuccess) return 1;
   if (grow(d.beg, d.beg_cap, ne + 1) != cudaSuccess) return 1;
   if (grow(d.scan_tmp, d.scan_tmp_cap, scan_tmp_entries(ne + 1)) != cudaSuccess) return 1;
@@ -651,9 +691,12 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
   Ent e;
   e.meta = b.cn_meta; e.child = b.cn_child; e.com = b.cn_com; e.spos = b.spos;
   e.quad = b.cn_quad; e.oct = b.cn_oct; e.rmax = d.rmax; e.n = n;
+  e.squad = p.order >= 4 ? d.squad : nullptr;
   const int lgrid = grid_for(n / 2 + 1, 256, 148 * 8);
   cudaMemsetAsync(d.cnt, 0, (ne + 1) * sizeof(int32_t), s);  // arrival counters (M < ne)
   rmax_fused_kernel<<<lgrid, 256, 0, s>>>(b.sc, e, b.cn_parent, d.rmax, d.cnt, &b.sc->err);
+  if (p.order >= 4)
+    spec_quad_kernel<<<lgrid, 256, 0, s>>>(b.sc, b.cn_com, b.cn_quad, d.squad);
 
   // counters: [0], [1] frontier sizes and [2], [3] mutual totals, each
   // alternating between generations; [4] overflow flags

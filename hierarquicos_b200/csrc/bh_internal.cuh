@@ -216,6 +216,8 @@ struct WalkParams {
 struct DehnenBuffers {
   double *rmax = nullptr, *F = nullptr, *H = nullptr, *T = nullptr;
   int64_t rmax_cap = 0, F_cap = 0, H_cap = 0, T_cap = 0;
+  double *squad = nullptr;                // every node's quadrupole over its mass
+  int64_t squad_cap = 0;
   int2 *front = nullptr, *mut = nullptr;
   int64_t front_cap = 0, mut_cap = 0;
   int64_t want_front = 0, want_mut = 0;   // pairs per frontier buffer, mutual pairs
