@@ -19,13 +19,23 @@
 // the whole build of a 2^20-body Hernquist system took 0.90-0.93 ms with it
 // (four block shapes) against 0.85 ms with these 22 launches, because each
 // thread's chain of dependent node loads up the tree serialises more than the
-// level launches do.
+// level launches do.  Small builds (a cooperative grid of at most half the
+// resident blocks, systems up to about 37,000 bodies) run all levels in one
+// cooperative launch with a grid barrier per level instead: there the level
+// launches cost more than their work.  At 2^20 the cooperative launch took
+// the build from 0.817 to 0.780 ms but cost the served rate 1 % (187.7 ->
+// 185.8 M forces/s): a cooperative grid waits until all of it fits, so it no
+// longer slips into the SMs that another lane's walk frees at its end.
 //
 // The same pass writes the normalised FP32 copies used by the FP32 walk:
 // quadrupole / (M ssa^2) with its trace, octupole / (M ssa^3), where M is the
 // total mass and ssa the root cube side, so the walk's values are O(1)
 // whatever the physical units.
+#include <cooperative_groups.h>
+
 #include "bh_internal.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace bh {
 
@@ -215,10 +225,78 @@ upward_level_kernel(int level, const int32_t *__restrict__ level_begin,
     compute_node<ORDER>(j, meta, child, spos, sys_of, sys, com, quad, oct, fq, fo);
 }
 
+// All levels in one cooperative launch: the grid takes every level's nodes
+// in turn, deepest first, with a grid-wide barrier after each level that has
+// nodes (the barrier also makes the level's writes visible to the next one,
+// which reads them through L2).  Same per-node arithmetic, so the same bits as
+// the per-level launches.
+template <int ORDER>
+__global__ void __launch_bounds__(128)
+upward_coop_kernel(const int32_t *__restrict__ level_begin, const int4 *__restrict__ meta,
+                   const int32_t *__restrict__ child, const double4 *__restrict__ spos,
+                   const int32_t *__restrict__ sys_of, const SysScalars *__restrict__ sys,
+                   double4 *com, double *quad, double *oct, float4 *__restrict__ fq,
+                   float4 *__restrict__ fo) {
+  cg::grid_group grid = cg::this_grid();
+  for (int level = kMaxDepth; level >= 0; --level) {
+    const int lb = level_begin[level], le = level_begin[level + 1];
+    if (lb >= le) continue;  // the same for every thread: no writes, no barrier
+    for (int j = lb + blockIdx.x * blockDim.x + threadIdx.x; j < le; j += gridDim.x * blockDim.x)
+      compute_node<ORDER>(j, meta, child, spos, sys_of, sys, com, quad, oct, fq, fo);
+    if (level > 0) grid.sync();
+  }
+}
+
+// Blocks of the cooperative launch that fit on the device at once (0: no
+// cooperative launch here), per device and order.
+template <int ORDER>
+int coop_blocks() {
+  static int per_dev[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (per_dev[dev] == 0) {
+    int coop = 0, sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, upward_coop_kernel<ORDER>, 128, 0);
+    per_dev[dev] = (coop && sms > 0 && per_sm > 0) ? per_sm * sms : -1;
+  }
+  return per_dev[dev] > 0 ? per_dev[dev] : 0;
+}
+
+template <int ORDER>
+bool launch_upward_coop(int64_t n, Buffers &b, cudaStream_t s) {
+  const int resident = coop_blocks<ORDER>();
+  if (resident <= 0) return false;
+  const int grid = grid_for(n / 2 + 1, 128, resident);
+  // a cooperative grid starts only when all of it fits: keep it to small
+  // builds, whose 22 level launches cost more than their work, and leave the
+  // large ones (which another stream's walk shares the GPU with) per level
+  if (2 * grid > resident) return false;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(128);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, upward_coop_kernel<ORDER>, (const int32_t *)b.level_begin,
+                            (const int4 *)b.cn_meta, (const int32_t *)b.cn_child,
+                            (const double4 *)b.spos, (const int32_t *)b.sys_of,
+                            (const SysScalars *)b.ss, b.cn_com, b.cn_quad, b.cn_oct, b.cn_fq,
+                            b.cn_fo) == cudaSuccess;
+}
+
 }  // namespace
 
 void launch_upward(int64_t n, int L, int order, Buffers &b, cudaStream_t s) {
   (void)L;
+  if (order >= 8 ? launch_upward_coop<8>(n, b, s)
+                 : (order >= 4 ? launch_upward_coop<4>(n, b, s) : launch_upward_coop<1>(n, b, s)))
+    return;
+  cudaGetLastError();  // a refused cooperative launch: the per-level launches instead
   const int grid = grid_for(n / 2 + 1, 128, 148 * 8);
   for (int level = kMaxDepth; level >= 0; --level) {
     if (order >= 8)
