@@ -174,8 +174,21 @@ int radix_sort_values32(uint32_t *k0, int32_t *v0, uint32_t *k1, int32_t *v1, in
 // 8192-value tile; scratch of the radix sort: digit counts of 8 passes x 256
 // digits, 8 tile counters, and a 64-bit word per (pass, 4096-key tile, digit)
 constexpr int64_t scan_tmp_entries(int64_t n) { return 2 * ((n + 8191) / 8192) + 4; }
+// radix sort tiles: sorts of at most kSortSmallMax keys use small tiles (more
+// blocks in flight: a 2^14-body build 0.380 -> 0.350 ms), larger ones large
+// tiles (fewer look-back words and less scratch to clear: with small tiles
+// the 2^20-body build took 0.873 instead of 0.821 ms)
+constexpr int64_t kSortTileLarge = 4096, kSortTileSmall = 1024, kSortSmallMax = (int64_t)1 << 16;
+constexpr int64_t sort_tile(int64_t n) { return n <= kSortSmallMax ? kSortTileSmall : kSortTileLarge; }
 constexpr int64_t radix_hist_entries(int64_t n) {
-  return 8 * 256 + 8 + 2 * 8 * 256 * ((n + 4095) / 4096 + 1);
+  // the most tiles any sort of up to n keys uses
+  return 8 * 256 + 8 +
+         2 * 8 * 256 *
+             ((((n < kSortSmallMax ? n : kSortSmallMax) + kSortTileSmall - 1) / kSortTileSmall >
+                       (n + kSortTileLarge - 1) / kSortTileLarge
+                   ? ((n < kSortSmallMax ? n : kSortSmallMax) + kSortTileSmall - 1) / kSortTileSmall
+                   : (n + kSortTileLarge - 1) / kSortTileLarge) +
+              1);
 }
 
 // exclusive scan of n int32 values in one launch; total written to *total

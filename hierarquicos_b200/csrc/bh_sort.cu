@@ -8,7 +8,8 @@
 //
 // Digit counts of every pass come from one histogram kernel over the keys;
 // each pass (8-bit digit) is then ONE kernel with decoupled look-back: a block
-// claims the next 4096-key tile from an atomic counter, ranks its keys inside
+// claims the next tile (4096 keys; 1024 for sorts of at most 65,536 keys, whose
+// few large tiles would leave most SMs idle) from an atomic counter, ranks its keys inside
 // the tile with warp __match_any_sync / popc ranking (element order = warp,
 // iteration, lane, so ranks are stable), publishes its per-digit counts, adds
 // up the counts of the tiles before it (each tile's word holds either its own
@@ -25,8 +26,9 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / kWarp;
-constexpr int kItems = 16;
-constexpr int kTile = kSortThreads * kItems;  // 4096 keys per block
+constexpr int kItems = 16;       // keys per thread of a large sort's tile
+constexpr int kSmallItems = kSortTileSmall / 256;  // and of a small sort's
+constexpr int kTile = kSortThreads * kItems;  // 4096 keys per block (large sorts)
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;  // 64-bit keys
 
@@ -126,10 +128,10 @@ __device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v) {
   asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-template <typename K>
+template <typename K, int ITEMS>
 struct PassSmem {
-  K sk[kTile];
-  int32_t sv[kTile];
+  K sk[ITEMS * kSortThreads];
+  int32_t sv[ITEMS * kSortThreads];
   int wh[kSortWarps][kRadix];
   int tile_start[kRadix];
   int gbase[kRadix];
@@ -139,14 +141,16 @@ struct PassSmem {
 
 // kout may be null: the pass then writes only the values (a last pass whose
 // keys nobody reads).
-template <typename K>
+template <typename K, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads)
 onesweep_kernel(const K *__restrict__ kin, const int32_t *__restrict__ vin,
                 K *__restrict__ kout, int32_t *__restrict__ vout, int64_t n_max,
                 const int32_t *n_dev, int shift, const uint32_t *__restrict__ gofs,
                 uint64_t *__restrict__ tiles, int32_t *__restrict__ tile_ctr, int *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  PassSmem<K> &S = *reinterpret_cast<PassSmem<K> *>(smem_raw);
+  PassSmem<K, ITEMS> &S = *reinterpret_cast<PassSmem<K, ITEMS> *>(smem_raw);
+  constexpr int kItems = ITEMS;
+  constexpr int kTile = ITEMS * kSortThreads;
   const int lane = threadIdx.x & (kWarp - 1), warp = threadIdx.x / kWarp;
   if (threadIdx.x == 0) S.tile = atomicAdd(tile_ctr, 1);
   for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&S.wh[0][0])[i] = 0;
@@ -337,11 +341,30 @@ regather_kernel(const uint64_t *__restrict__ k0, const int32_t *__restrict__ v0,
   }
 }
 
-bool g_sort_attr_set[2] = {false, false};
+template <typename K, int ITEMS>
+void set_pass_smem() {
+  static bool done = false;  // a function attribute: once per process
+  if (!done) {
+    cudaFuncSetAttribute(onesweep_kernel<K, ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PassSmem<K, ITEMS>));
+    done = true;
+  }
+}
+
+template <typename K, int ITEMS>
+void launch_pass(int64_t ntiles, const K *ki, const int32_t *vi, K *ko, int32_t *vo, int64_t n,
+                 const int32_t *n_dev, int shift, const uint32_t *gofs, uint64_t *tiles,
+                 int32_t *ctr, int *err, cudaStream_t s) {
+  set_pass_smem<K, ITEMS>();
+  onesweep_kernel<K, ITEMS><<<(unsigned)(ntiles > 0 ? ntiles : 1), kSortThreads,
+                              sizeof(PassSmem<K, ITEMS>), s>>>(ki, vi, ko, vo, n, n_dev, shift,
+                                                               gofs, tiles, ctr, err);
+}
 
 }  // namespace
 
-static_assert(kScanChunk == 8192 && kTile == 4096 && kRadix == 256 && kMaxPasses == 8,
+static_assert(kScanChunk == 8192 && kTile == kSortTileLarge && kRadix == 256 && kMaxPasses == 8 &&
+                  kSortThreads * kSmallItems == kSortTileSmall,
               "scan_tmp_entries / radix_hist_entries in bh_internal.cuh assume these sizes");
 
 void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n_dev,
@@ -357,13 +380,9 @@ void exclusive_scan(const int32_t *in, int32_t *out, int64_t n, const int32_t *n
 template <typename K>
 static int sort_passes(K *k0, int32_t *v0, K *k1, int32_t *v1, int64_t n, const int32_t *n_dev,
                        int bits, int32_t *hist, int *err, bool keys_out, cudaStream_t s) {
-  bool &attr = g_sort_attr_set[sizeof(K) == 8 ? 1 : 0];
-  if (!attr) {
-    cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PassSmem<K>));
-    attr = true;
-  }
-  const int64_t ntiles = (n + kTile - 1) / kTile;
+  // small sorts take small tiles: more blocks in flight for the same keys
+  const int64_t tile = sort_tile(n);
+  const int64_t ntiles = (n + tile - 1) / tile;
   int passes = (bits + 7) / 8;
   if (passes < 1) passes = 1;
   if (passes > (int)sizeof(K)) passes = (int)sizeof(K);
@@ -381,9 +400,12 @@ static int sort_passes(K *k0, int32_t *v0, K *k1, int32_t *v1, int64_t n, const 
   int32_t *vi = v0, *vo = v1;
   for (int p = 0; p < passes; ++p) {
     K *kw = (p == passes - 1 && !keys_out) ? nullptr : ko;
-    onesweep_kernel<K><<<(unsigned)(ntiles > 0 ? ntiles : 1), kSortThreads, sizeof(PassSmem<K>),
-                         s>>>(ki, vi, kw, vo, n, n_dev, 8 * p, ghist + p * kRadix,
-                              tiles + (int64_t)p * ntiles * kRadix, ctr + p, err);
+    if (tile == kSortTileSmall)
+      launch_pass<K, kSmallItems>(ntiles, ki, vi, kw, vo, n, n_dev, 8 * p, ghist + p * kRadix,
+                                  tiles + (int64_t)p * ntiles * kRadix, ctr + p, err, s);
+    else
+      launch_pass<K, kItems>(ntiles, ki, vi, kw, vo, n, n_dev, 8 * p, ghist + p * kRadix,
+                             tiles + (int64_t)p * ntiles * kRadix, ctr + p, err, s);
     K *tk = ki; ki = ko; ko = tk;
     int32_t *tv = vi; vi = vo; vo = tv;
   }
