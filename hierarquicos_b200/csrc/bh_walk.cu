@@ -36,7 +36,12 @@ namespace {
 // The walk runs one warp per block.  The FP32 walk is compiled for 16 resident
 // blocks per SM (128 registers a thread).
 constexpr int kWalkBlocksPerSm = 16;
-template <typename T> constexpr int walk_min_blocks() { return sizeof(T) == 4 ? kWalkBlocksPerSm : 1; }
+// One-warp blocks per SM the walk is compiled for, FP64 as FP32: 16 (128
+// registers) against the compiler's own choice for FP64 (182 / 222 registers,
+// 11 / 9 warps per SM) took the FP64 walk at 2^20 from 15.5 to 12.3 ms
+// (quadrupole) and from 29.4 to 26.3 ms (octupole, despite 592 bytes of
+// spills; 12 blocks: 27.1 ms), the same bits.
+template <typename T, int ORDER> constexpr int walk_min_blocks() { return kWalkBlocksPerSm; }
 constexpr int kCellQ = 64;
 constexpr int kBodyPerLane = 16;
 constexpr int kBodyQ = 32 + kWarp * kBodyPerLane;  // 544
@@ -758,7 +763,7 @@ __device__ __forceinline__ void walk_group(const WalkArgs &a, WarpSmem<T, ORDER>
 // none is left; block b uses stack slot b.  With 64-body groups a group of
 // <= 32 bodies runs the one-target-per-lane path.
 template <typename T, int ORDER, int MAXTPL, bool SOFT>
-__global__ void __launch_bounds__(kWarp, walk_min_blocks<T>())
+__global__ void __launch_bounds__(kWarp, walk_min_blocks<T, ORDER>())
 group_walk_kernel(WalkArgs a) {
   __shared__ WarpSmem<T, ORDER> S;
   const int lane = threadIdx.x;
