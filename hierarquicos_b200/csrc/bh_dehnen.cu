@@ -751,8 +751,9 @@ int run_dehnen(int64_t n, const WalkParams &p, Buffers &b, DehnenBuffers &d, dou
     expand_kernel<<<g, 256, 0, s>>>(d.mut, np, reinterpret_cast<uint2 *>(d.keys),
                                     reinterpret_cast<int2 *>(d.vals), d.cnt);
     // stable by target: a target's terms keep the mutual list's order
+    // the digit counts come from the terms per target that expand counted
     if (radix_sort_values32(d.keys, d.vals, d.keys + nh, d.vals + nh, nh, bits_for64(ne), d.hist,
-                            &b.sc->err, s) == 1)
+                            &b.sc->err, s, d.cnt, ne) == 1)
       sources = d.vals + nh;
   }
   exclusive_scan(d.cnt, d.beg, ne + 1, nullptr, nullptr, d.scan_tmp, &b.sc->err, s);

@@ -167,9 +167,12 @@ void radix_sort_pairs(uint64_t *k0, int32_t *v0, uint64_t *k1, int32_t *v1, int6
                       const int32_t *n_dev, int bits, int32_t *hist, int *err, cudaStream_t s);
 // the same for 32-bit keys when only the values are wanted: the last pass
 // writes no keys and nothing is copied back; returns the buffer holding the
-// sorted values (0: v0, 1: v1)
+// sorted values (0: v0, 1: v1).  key_counts, if given, holds the number of keys
+// of every key value 0..n_key_values-1 (the digit counts then come from it
+// instead of from a pass over the keys).
 int radix_sort_values32(uint32_t *k0, int32_t *v0, uint32_t *k1, int32_t *v1, int64_t n, int bits,
-                        int32_t *hist, int *err, cudaStream_t s);
+                        int32_t *hist, int *err, cudaStream_t s,
+                        const int32_t *key_counts = nullptr, int64_t n_key_values = 0);
 // scratch of the scan, in int32 entries: a ticket and a 64-bit word per
 // 8192-value tile; scratch of the radix sort: digit counts of 8 passes x 256
 // digits, 8 tile counters, and a 64-bit word per (pass, 4096-key tile, digit)
