@@ -540,6 +540,28 @@ def run_ours(args):
             b.synchronize()
             te.append(a.elapsed_time(b))
         plain_e2e_ms = dist_max(statistics.mean(te), dev, world)
+        # the host link itself on this box: the call's four input copies
+        # (pinned, 32 B/body) and its result copy (24 B/body) alone
+        dstage = torch.empty(4 * n, dtype=torch.float64, device=dev)
+
+        def link(fn):
+            ts = []
+            for i in range(W + K):
+                torch.cuda.synchronize()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                if i >= W:
+                    ts.append(a.elapsed_time(b))
+            return statistics.median(ts)
+
+        h2d_ms = link(lambda: [dstage[k * n:(k + 1) * n].copy_(h, non_blocking=True)
+                               for k, h in enumerate((hm, hx, hy, hz))])
+        d2h_ms = link(lambda: hout.copy_(dstage[:3 * n], non_blocking=True))
+        del dstage
         # the api3d drop-in from ordinary (pageable) numpy arrays, as the
         # reference's f2py callers pass them: a fresh Fortran-ordered result
         # array per call, as the f2py function returns
@@ -581,6 +603,10 @@ def run_ours(args):
                        "host_cpus": bound_cpus,
                        "p50_ms": hmet["p50_ms"], "p99_ms": hmet["p99_ms"],
                        "equal_to_plain_bitwise": same_host,
+                       "host_link": {"h2d_ms": h2d_ms, "h2d_GBps": 32 * n / (h2d_ms * 1e6),
+                                     "d2h_ms": d2h_ms, "d2h_GBps": 24 * n / (d2h_ms * 1e6),
+                                     "note": "the plain call's own copies, timed alone on this "
+                                             "box: its floor is the device step plus both"},
                        "plain": {"value": world * n / (plain_e2e_ms * 1e-3), "ms_per_step": plain_e2e_ms,
                                  "ms_min": min(te), "ms_median": statistics.median(te),
                                  "ms_max": max(te),
