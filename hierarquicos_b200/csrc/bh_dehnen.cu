@@ -408,8 +408,12 @@ expand_kernel(const int2 *__restrict__ mut, int64_t np, uint2 *__restrict__ keys
     const int32_t a = mut[i].x, b = mut[i].y;
     keys[i] = make_uint2((uint32_t)a, (uint32_t)b);  // terms 2i (a <- b) and 2i + 1 (b <- a)
     vals[i] = make_int2(b, a);
-    atomicAdd(&cnt[a], 1);
-    atomicAdd(&cnt[b], 1);
+    // one add per distinct target in the warp (consecutive mutual pairs often
+    // share a member): 13.9 -> 13.6-13.8 ms per call at 2^20
+    const unsigned act = __activemask(), lt = (1u << (threadIdx.x & 31)) - 1u;
+    const unsigned pa = __match_any_sync(act, a), pb = __match_any_sync(act, b);
+    if ((pa & lt) == 0) atomicAdd(&cnt[a], __popc(pa));
+    if ((pb & lt) == 0) atomicAdd(&cnt[b], __popc(pb));
   }
 }
 
@@ -493,13 +497,15 @@ __device__ __forceinline__ void add_term(const Ent &e, int64_t t, const double4 
 }
 
 // Sum of the one-sided terms of every target, kEvalLanes lanes per target
-// (four targets per warp): lane l of a target's group adds terms l, l + 8, ...
+// (two targets per warp): lane l of a target's group adds terms l, l + 16, ...
 // of the target's list (in the mutual list's deterministic order), then the
 // group's sums are combined by a fixed butterfly, so the result depends only
-// on the target's own list.  Eight lanes rather than the whole warp: a target
-// has about a hundred terms, and a 19-value butterfly over 32 lanes per target
-// costs about a fifth of the evaluation.
-constexpr int kEvalLanes = 8;
+// on the target's own list.  A target has about a hundred terms; at 2^20 the
+// quadrupole call took 14.6 / 14.2 / 14.0 / 14.7 ms with 4 / 8 / 16 / 32 lanes
+// per target (the octupole 17.1 ms with 8, 16.8 with 16, 17.7 with 32): fewer
+// lanes leave each lane a longer chain of loads, more make the butterfly over
+// the 19-22 sums a larger share.
+constexpr int kEvalLanes = 16;
 
 template <int ORDER>
 __global__ void __launch_bounds__(128)
