@@ -266,6 +266,12 @@ int coop_blocks() {
 
 template <int ORDER>
 bool launch_upward_coop(int64_t n, Buffers &b, cudaStream_t s) {
+  // inside a graph capture the level launches cost little (the graph launches
+  // them back to back), and a graph holding a cooperative node is slower to
+  // set up: keep the per-level form there
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return false;
   const int resident = coop_blocks<ORDER>();
   if (resident <= 0) return false;
   const int grid = grid_for(n / 2 + 1, 128, resident);
