@@ -110,7 +110,7 @@ class ForceField:
             # the graph writes into the field's own buffer (callers often hand
             # a fresh output per call), copied out afterwards
             key = (st.m.data_ptr(), x.data_ptr(), y.data_ptr(), z.data_ptr(), st.n,
-                   st.offsets.tobytes())
+                   st.offsets.tobytes(), bytes(self.params))  # changed parameters record anew
             if key == self._graph_key:
                 try:
                     self.sys.replay()

@@ -163,6 +163,19 @@ def test_graph_replayed_field_follows_the_plain_trajectory(ig):
     for (qa, pa), (qb, pb) in zip(*ends):
         assert np.array_equal(qa, qb) and np.array_equal(pa, pb)
 
+    # parameters changed between calls are recorded anew, not replayed stale
+    import torch
+
+    one = ig.BatchState.single(m, q.T, p.T)
+    field = ig.ForceField("bh", theta=0.8, eps=0.01, order=1, graph=True)
+    f = torch.empty(3 * one.n, dtype=torch.float64, device=one.device)
+    field(one, f)
+    field(one, f)  # replayed
+    field.params.theta = 0.4
+    field(one, f)
+    ref = ig.ForceField("bh", theta=0.4, eps=0.01, order=1)(one, torch.empty_like(f))
+    assert torch.equal(f, ref)
+
 
 def test_parareal_matches_oracle_direct(ig, oracle_mod):
     """The reference's Parareal with direct-force propagators, device against
